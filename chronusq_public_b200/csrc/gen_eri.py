@@ -1,0 +1,366 @@
+"""Generate the per-class McMurchie-Davidson ERI device functions.
+
+For every shell-quartet class (la lb | lc ld) with la >= lb, lc >= ld and the bra pair
+class not below the ket pair class, this emits one fully unrolled device function
+
+    template <typename T>
+    __device__ void eri_<la><lb><lc><ld>(const PrimPair* bra, int nbra,
+                                         const PrimPair* ket, int nket,
+                                         double3 A, double3 B, double3 C, double3 D,
+                                         const double* boys_tab, T* out)
+
+that returns the contracted, normalised (ab|cd) over the reference's basis functions
+(spherical for pure shells) in row-major [a][b][c][d] order.
+
+Method (McMurchie & Davidson, J. Comput. Phys. 26, 218 (1978); notation of Helgaker,
+Jorgensen & Olsen ch. 9.5 and 9.9):
+
+  (ab|cd) = sum_prims  2 pi^(5/2) / (p q sqrt(p+q)) K_ab K_cd
+            sum_tuv E^ab_tuv sum_tau,nu,phi (-1)^(tau+nu+phi) E^cd_tau,nu,phi R_(t+tau,u+nu,v+phi)
+
+The ket Hermite sum is accumulated over ket primitive pairs into W[tuv][cd] for one bra
+primitive pair, and the bra Hermite transform is applied once per bra primitive pair.
+E coefficients are built per primitive pair by the 1D recursion; R by the standard
+downward recursion on n from R^n_000 = (-2 rho)^n F_n(rho |PQ|^2).  Boys values come
+from :file:`boys.cuh` in FP64 regardless of ``T``; everything after them runs in ``T``.
+
+Run:  python gen_eri.py <out.cuh> [maxl]
+"""
+import itertools
+import sys
+from math import comb, sqrt, floor
+
+import numpy as np
+
+
+def cart_list(l):
+    out = []
+    for i in range(l + 1):
+        for j in range(i + 1):
+            out.append((l - i, i - j, j))
+    return out
+
+
+def herm_list(n):
+    """(t,u,v) with t+u+v <= n, ordered by total then CCA order."""
+    out = []
+    for L in range(n + 1):
+        out.extend(cart_list(L))
+    return out
+
+
+def _dfact(n):
+    r = 1.0
+    while n > 1:
+        r *= n
+        n -= 2
+    return r
+
+
+def solid_harmonic_matrix(l):
+    """Rows m=-l..l of unit-normalised real solid harmonics (x^l-normalised Cartesians).
+    Same construction as chronusq_public_b200.basis.solid_harmonic_matrix (Helgaker eqs.
+    6.4.47-6.4.50), duplicated so the generator has no package import."""
+    carts = cart_list(l)
+    idx = {c: k for k, c in enumerate(carts)}
+    mat = np.zeros((2 * l + 1, len(carts)))
+    for m in range(-l, l + 1):
+        am = abs(m)
+        vm = 0.0 if m >= 0 else 0.5
+        row = np.zeros(len(carts))
+        for t in range((l - am) // 2 + 1):
+            for u in range(t + 1):
+                nv = int(floor(am / 2.0 - vm))
+                for iv in range(nv + 1):
+                    v = iv + vm
+                    two_v = int(round(2 * v))
+                    sign = (-1.0) ** int(round(t + v - vm))
+                    c = (sign * 0.25 ** t * comb(l, t) * comb(l - t, am + t) * comb(t, u) * comb(am, two_v))
+                    row[idx[(2 * t + am - 2 * u - two_v, 2 * u + two_v, l - 2 * t - am)]] += c
+        gram = np.zeros((len(carts), len(carts)))
+        for a, (ax, ay, az) in enumerate(carts):
+            for b, (bx, by, bz) in enumerate(carts):
+                sx, sy, sz = ax + bx, ay + by, az + bz
+                if sx % 2 or sy % 2 or sz % 2:
+                    continue
+                gram[a, b] = _dfact(sx - 1) * _dfact(sy - 1) * _dfact(sz - 1) / _dfact(2 * l - 1)
+        mat[m + l] = row / sqrt(float(row @ gram @ row))
+    return mat
+
+
+def lit(x):
+    r = repr(float(x))
+    return "T(%s)" % r
+
+
+class Gen:
+    def __init__(self):
+        self.lines = []
+        self.ind = 1
+
+    def w(self, s):
+        self.lines.append("  " * self.ind + s)
+
+
+def emit_E(g, tag, la, lb, need):
+    """Emit 1D Hermite coefficients E{tag}{dir}_{i}_{j}_{t} for dir in x,y,z.
+    Variables used: {tag}PA{d}, {tag}PB{d}, {tag}o2p (=1/(2p)).  Only (i,j) in `need[d]`
+    plus their recursion predecessors are emitted."""
+    names = {}
+    for d in "xyz":
+        # closure of needed (i,j)
+        req = set()
+        stack = list(need[d])
+        while stack:
+            ij = stack.pop()
+            if ij in req:
+                continue
+            req.add(ij)
+            i, j = ij
+            if i > 0:
+                stack.append((i - 1, j))
+            elif j > 0:
+                stack.append((i, j - 1))
+        order = sorted(req, key=lambda x: (x[0] + x[1], x[0]))
+        for (i, j) in order:
+            for t in range(i + j + 1):
+                nm = "E%s%s_%d_%d_%d" % (tag, d, i, j, t)
+                names[(d, i, j, t)] = nm
+                if i == 0 and j == 0:
+                    continue  # E_0_0_0 = 1 handled symbolically
+                if i > 0:
+                    pi, pj, X = i - 1, j, "%sPA%s" % (tag, d)
+                else:
+                    pi, pj, X = i, j - 1, "%sPB%s" % (tag, d)
+                terms = []
+
+                def ref(tt):
+                    if tt < 0 or tt > pi + pj:
+                        return None
+                    if pi == 0 and pj == 0:
+                        return "T(1)" if tt == 0 else None
+                    return "E%s%s_%d_%d_%d" % (tag, d, pi, pj, tt)
+                a = ref(t - 1)
+                if a:
+                    terms.append("%so2p * %s" % (tag, a) if a != "T(1)" else "%so2p" % tag)
+                b = ref(t)
+                if b:
+                    terms.append("%s * %s" % (X, b) if b != "T(1)" else X)
+                c = ref(t + 1)
+                if c:
+                    terms.append("T(%d) * %s" % (t + 1, c) if t + 1 > 1 else c)
+                g.w("const T %s = %s;" % (nm, " + ".join(terms) if terms else "T(0)"))
+    return names
+
+
+def Ename(tag, d, i, j, t):
+    if i == 0 and j == 0:
+        return None  # equals 1
+    return "E%s%s_%d_%d_%d" % (tag, d, i, j, t)
+
+
+def herm_terms(tag, ca, cb):
+    """List of ((t,u,v), [factor names]) for the Hermite expansion of Cartesian pair."""
+    out = []
+    rngs = [range(ca[k] + cb[k] + 1) for k in range(3)]
+    for t in rngs[0]:
+        for u in rngs[1]:
+            for v in rngs[2]:
+                fac = []
+                for d, (i, j, tt) in zip("xyz", ((ca[0], cb[0], t), (ca[1], cb[1], u), (ca[2], cb[2], v))):
+                    nm = Ename(tag, d, i, j, tt)
+                    if nm:
+                        fac.append(nm)
+                out.append(((t, u, v), fac))
+    return out
+
+
+def gen_class(la, lb, lc, ld, pa, pb, pc, pd):
+    L = la + lb + lc + ld
+    p_l = la + lb
+    q_l = lc + ld
+    ca, cb, cc, cd = cart_list(la), cart_list(lb), cart_list(lc), cart_list(ld)
+    nab, ncd = len(ca) * len(cb), len(cc) * len(cd)
+    hp = herm_list(p_l)
+    hidx = {h: k for k, h in enumerate(hp)}
+    name = "eri_%d%d%d%d" % (la, lb, lc, ld)
+    g = Gen()
+    g.lines.append("template <typename T>")
+    g.lines.append("__device__ __forceinline__ void %s(const PrimPair* __restrict__ bra, int nbra,"
+                   " const PrimPair* __restrict__ ket, int nket, double3 A, double3 B, double3 C,"
+                   " double3 D, const double* __restrict__ boys_tab, T* __restrict__ out) {" % name)
+    for i in range(nab * ncd):
+        g.w("T acc%d = T(0);" % i)
+    g.w("for (int ib = 0; ib < nbra; ++ib) {")
+    g.ind += 1
+    g.w("const PrimPair pb = bra[ib];")
+    g.w("const double p = pb.p;")
+    g.w("const T bo2p = T(0.5 / p);")
+    for d, comp in zip("xyz", "xyz"):
+        g.w("const T bPA%s = T(pb.P%s - A.%s);" % (d, comp, comp))
+        g.w("const T bPB%s = T(pb.P%s - B.%s);" % (d, comp, comp))
+    needb = {d: set() for d in "xyz"}
+    for a in ca:
+        for b in cb:
+            for k, d in enumerate("xyz"):
+                needb[d].add((a[k], b[k]))
+    emit_E(g, "b", la, lb, needb)
+    for h in range(len(hp)):
+        for c in range(ncd):
+            g.w("T W%d_%d = T(0);" % (h, c))
+    g.w("for (int ik = 0; ik < nket; ++ik) {")
+    g.ind += 1
+    g.w("const PrimPair pk = ket[ik];")
+    g.w("const double q = pk.p;")
+    g.w("const T ko2p = T(0.5 / q);")
+    for d in "xyz":
+        g.w("const T kPA%s = T(pk.P%s - C.%s);" % (d, d, d))
+        g.w("const T kPB%s = T(pk.P%s - D.%s);" % (d, d, d))
+    needk = {d: set() for d in "xyz"}
+    for c in cc:
+        for dd in cd:
+            for k, d in enumerate("xyz"):
+                needk[d].add((c[k], dd[k]))
+    emit_E(g, "k", lc, ld, needk)
+    g.w("const double pq = p + q;")
+    g.w("const double rho = p * q / pq;")
+    g.w("const double PQx = pb.Px - pk.Px, PQy = pb.Py - pk.Py, PQz = pb.Pz - pk.Pz;")
+    g.w("const double Tb = rho * (PQx * PQx + PQy * PQy + PQz * PQz);")
+    g.w("double F[%d];" % (L + 1))
+    g.w("boys_eval<%d>(Tb, boys_tab, F);" % L)
+    g.w("const double pref = TWO_PI_2P5 / (p * q * sqrt(pq)) * pb.K * pk.K;")
+    # R^n_000
+    g.w("const double m2r = -2.0 * rho;")
+    g.w("double fac = pref;")
+    for n in range(L + 1):
+        g.w("const T R%d_0_0_0 = T(fac * F[%d]);" % (n, n))
+        if n < L:
+            g.w("fac *= m2r;")
+    g.w("const T Xpq = T(PQx), Ypq = T(PQy), Zpq = T(PQz);")
+    # recursion: R^n_{tuv} for t+u+v <= L-n, from n = L-1 down to 0
+    # need R^0_{tuv} for t+u+v <= L only for those used; emit all (dead code eliminated)
+    defined = set((n, 0, 0, 0) for n in range(L + 1))
+    for n in range(L - 1, -1, -1):
+        for tot in range(1, L - n + 1):
+            for (t, u, v) in cart_list(tot):
+                if t > 0:
+                    a = "R%d_%d_%d_%d" % (n + 1, t - 1, u, v)
+                    b = ("R%d_%d_%d_%d" % (n + 1, t - 2, u, v)) if t > 1 else None
+                    expr = "Xpq * %s" % a + ((" + T(%d) * %s" % (t - 1, b)) if b else "")
+                elif u > 0:
+                    a = "R%d_%d_%d_%d" % (n + 1, t, u - 1, v)
+                    b = ("R%d_%d_%d_%d" % (n + 1, t, u - 2, v)) if u > 1 else None
+                    expr = "Ypq * %s" % a + ((" + T(%d) * %s" % (u - 1, b)) if b else "")
+                else:
+                    a = "R%d_%d_%d_%d" % (n + 1, t, u, v - 1)
+                    b = ("R%d_%d_%d_%d" % (n + 1, t, u, v - 2)) if v > 1 else None
+                    expr = "Zpq * %s" % a + ((" + T(%d) * %s" % (v - 1, b)) if b else "")
+                g.w("const T R%d_%d_%d_%d = %s;" % (n, t, u, v, expr))
+    # ket transform: W[tuv][cd] += sum_{tau nu phi} (-1)^(..) Ecd * R0_{t+tau,...}
+    ci = 0
+    for c in cc:
+        for dd in cd:
+            for (tnp, fac) in herm_terms("k", c, dd):
+                sgn = -1 if (sum(tnp) % 2) else 1
+                coef = " * ".join(fac) if fac else None
+                cname = "kc_%d_%d_%d_%d" % (ci, tnp[0], tnp[1], tnp[2])
+                if coef is None:
+                    cexpr = "T(%d)" % sgn
+                else:
+                    cexpr = ("-" if sgn < 0 else "") + "(" + coef + ")"
+                g.w("{ const T %s = %s;" % (cname, cexpr))
+                for hi, (t, u, v) in enumerate(hp):
+                    g.w("  W%d_%d += %s * R0_%d_%d_%d;" % (hi, ci, cname, t + tnp[0], u + tnp[1], v + tnp[2]))
+                g.w("}")
+            ci += 1
+    g.ind -= 1
+    g.w("}")
+    # bra transform: acc[ab][cd] += sum_tuv Eab_tuv W[tuv][cd]
+    ai = 0
+    for a in ca:
+        for b in cb:
+            for (tuv, fac) in herm_terms("b", a, b):
+                hi = hidx[tuv]
+                coef = " * ".join(fac) if fac else "T(1)"
+                g.w("{ const T bc = %s;" % coef)
+                for c in range(ncd):
+                    g.w("  acc%d += bc * W%d_%d;" % (ai * ncd + c, hi, c))
+                g.w("}")
+            ai += 1
+    g.ind -= 1
+    g.w("}")
+    # spherical transform, axis by axis: cart arrays named by index tuples
+    dims = [len(ca), len(cb), len(cc), len(cd)]
+    pures = [pa, pb, pc, pd]
+    ls = [la, lb, lc, ld]
+    cur = {}
+    for idx in itertools.product(*[range(x) for x in dims]):
+        flat = ((idx[0] * dims[1] + idx[1]) * dims[2] + idx[2]) * dims[3] + idx[3]
+        cur[idx] = "acc%d" % flat
+    stage = 0
+    for ax in range(4):
+        if not pures[ax]:
+            continue
+        M = solid_harmonic_matrix(ls[ax])
+        ns = 2 * ls[ax] + 1
+        newdims = list(dims)
+        newdims[ax] = ns
+        new = {}
+        for idx in itertools.product(*[range(x) for x in newdims]):
+            terms = []
+            for k in range(dims[ax]):
+                cval = M[idx[ax], k]
+                if abs(cval) < 1e-15:
+                    continue
+                src = list(idx)
+                src[ax] = k
+                terms.append("%s * %s" % (lit(cval), cur[tuple(src)]))
+            nm = "s%d_%s" % (stage, "_".join(map(str, idx)))
+            g.w("const T %s = %s;" % (nm, " + ".join(terms) if terms else "T(0)"))
+            new[idx] = nm
+        cur = new
+        dims = newdims
+        stage += 1
+    for idx in itertools.product(*[range(x) for x in dims]):
+        flat = ((idx[0] * dims[1] + idx[1]) * dims[2] + idx[2]) * dims[3] + idx[3]
+        g.w("out[%d] = %s;" % (flat, cur[idx]))
+    g.lines.append("}")
+    return name, "\n".join(g.lines)
+
+
+def pair_classes(maxl):
+    return [(a, b) for a in range(maxl + 1) for b in range(a + 1)]
+
+
+def quartet_classes(maxl):
+    pcs = pair_classes(maxl)
+    out = []
+    for i, P in enumerate(pcs):
+        for j, Qc in enumerate(pcs):
+            if j <= i:
+                out.append((P[0], P[1], Qc[0], Qc[1]))
+    return out
+
+
+def main(path, maxl=2):
+    parts = ["// GENERATED by gen_eri.py -- do not edit.",
+             "#pragma once",
+             "#include \"../eri_common.cuh\"",
+             ""]
+    for (la, lb, lc, ld) in quartet_classes(maxl):
+        _, code = gen_class(la, lb, lc, ld, la > 1, lb > 1, lc > 1, ld > 1)
+        parts.append(code)
+        parts.append("template <> struct EriClass<%d, %d, %d, %d> {" % (la, lb, lc, ld))
+        parts.append("  template <typename T> static __device__ __forceinline__ void run(const PrimPair* bra, int nbra,"
+                     " const PrimPair* ket, int nket, double3 A, double3 B, double3 C, double3 D,"
+                     " const double* boys_tab, T* out) {")
+        parts.append("    eri_%d%d%d%d<T>(bra, nbra, ket, nket, A, B, C, D, boys_tab, out);" % (la, lb, lc, ld))
+        parts.append("  }")
+        parts.append("};")
+        parts.append("")
+    with open(path, "w") as f:
+        f.write("\n".join(parts))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1], int(sys.argv[2]) if len(sys.argv) > 2 else 2)

@@ -1,0 +1,127 @@
+/*
+ * cqgpu: B200 (sm_100a) direct-SCF two-electron engine -- C ABI.
+ *
+ * Drop-in for ChronusQ's AOIntegrals direct two-electron contraction.  Every matrix is
+ * real FP64, nbf x nbf, column-major with leading dimension `ld` (>= nbf), basis
+ * functions ordered as the reference orders them: atom order, then the .gbs shell
+ * order (SP split S then P), then components (Cartesian x^l, x^(l-1)y, x^(l-1)z, ...;
+ * real solid harmonics m=-l..l for pure shells).  Results ACCUMULATE into AX (AX +=),
+ * as the reference does; callers zero AX first when they want G alone.
+ *
+ * Pointers are host pointers when `on_device` is 0 (the call copies in and out on
+ * `stream`, and returns after the copy-out has completed) and device pointers of the
+ * context's device when `on_device` is 1 (the call only enqueues work on `stream`).
+ * `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *
+ * Errors are returned as cqg_status; nothing aborts or traps on the device.
+ * A context is not safe for concurrent use from several threads.
+ */
+#ifndef CQGPU_H
+#define CQGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  CQG_OK = 0,
+  CQG_ERR_BAD_ARG = 1,       /* reference: assert on list sizes (aointegrals_contract.h:31-33) */
+  CQG_ERR_OOM = 2,           /* reference: std::bad_alloc from CQMemManager (memory.h:65-88) */
+  CQG_ERR_CUDA = 3,          /* a CUDA runtime call failed */
+  CQG_ERR_TIMEOUT = 4,       /* a bounded device wait gave up */
+  CQG_ERR_NONFINITE = 5,     /* NaN/Inf found in an input density */
+  CQG_ERR_STATE = 6,         /* call order violated (e.g. contraction before basis) */
+  CQG_ERR_UNSUPPORTED = 7    /* outside what this engine implements (see cqg_last_error) */
+} cqg_status;
+
+/* ERI_CONTRACTION_TYPE (include/aointegrals.h:468-472) */
+enum { CQG_COULOMB = 0, CQG_EXCHANGE = 1 };
+
+/* precision policy of the quartet evaluation */
+enum {
+  CQG_PREC_FP64 = 0,         /* every quartet in FP64 (the reference's arithmetic) */
+  CQG_PREC_MIXED = 1         /* quartets whose Schwarz product Q_ab*Q_cd is below the
+                                FP32 cutoff are evaluated in FP32, accumulated in FP64 */
+};
+
+typedef struct cqg_ctx cqg_ctx;
+
+/* statistics of the last contraction on a context */
+typedef struct {
+  long long quartets;              /* screened unique shell quartets (the unit of work) */
+  long long quartets_fp32;         /* of which evaluated in FP32 (mixed policy) */
+  long long prim_quartets;         /* primitive quartets evaluated */
+  double model_flops;              /* MD-v1 model FLOPs of the screened quartets */
+  double ms_screen;                /* device time of screening + list build (ms) */
+  double ms_eri;                   /* device time of ERI + digest kernels (ms) */
+  double ms_total;                 /* device time of the whole call (ms) */
+  long long class_quartets[55];    /* per quartet class (index: see cqg_class_name) */
+  double class_ms[55];             /* device time per class kernel (ms), if timing on */
+} cqg_stats;
+
+/* Library / context lifetime. */
+const char *cqg_version(void);
+const char *cqg_status_string(cqg_status s);
+cqg_status cqg_create(cqg_ctx **ctx, int device);
+cqg_status cqg_destroy(cqg_ctx *ctx);
+const char *cqg_last_error(const cqg_ctx *ctx);
+
+/* Basis upload (replaces BasisSet::shells_ + mapSh2Bf, include/basisset.h;
+ * src/basisset/basisset_map.cpp:29-40).  Per shell: angular momentum L, pure flag
+ * (1 = spherical; the engine requires pure == (L > 1), the reference default at
+ * src/basisset/basisset_read.cpp:250-251), primitive count; alpha/coef are the
+ * concatenated exponents and NORMALISED contraction coefficients (as held by a
+ * libint2::Shell after renormShells, src/basisset/basisset_misc.cpp:95-111);
+ * centers is nshell x 3 in bohr.  Computes the Schwarz bounds on the device
+ * (AOIntegrals::computeSchwartz, src/aointegrals/aointegrals_builders.cpp:469-517). */
+cqg_status cqg_set_basis(cqg_ctx *ctx, int nshell, const int *L, const int *pure,
+                         const int *nprim, const double *alpha, const double *coef,
+                         const double *centers);
+
+/* AOIntegrals::thresholdSchwartz_ (include/aointegrals.h:334; default 1e-14). */
+cqg_status cqg_set_threshold(cqg_ctx *ctx, double thresh);
+
+/* Precision policy; `fp32_cutoff` is the Schwarz-product cutoff for CQG_PREC_MIXED. */
+cqg_status cqg_set_precision(cqg_ctx *ctx, int policy, double fp32_cutoff);
+
+/* Copy the nshell x nshell Schwarz matrix (column-major) to host memory. */
+cqg_status cqg_get_schwarz(cqg_ctx *ctx, double *Q);
+cqg_status cqg_get_sizes(cqg_ctx *ctx, int *nshell, int *nbasis, int *maxl);
+
+/* AOIntegrals::newTwoEContractDirect (include/aointegrals/aointegrals_contract.h:24-194,
+ * declared include/aointegrals.h:474-480) for real matrices:
+ *   for i < nmat:  AX[i] += 0.5 * scale[i] * G_i[X[i]]
+ * with G = 4 J[X] for types[i] == CQG_COULOMB and G = 4 K[X] for CQG_EXCHANGE (so
+ * AX += scale * 2J or scale * 2K), J_mn = sum (mn|ls) X_ls, K_mn = sum (ml|ns) X_ls,
+ * over the unique shell quartets that pass the reference's density-weighted Schwarz
+ * screen.  X must be symmetric (the engine checks and returns CQG_ERR_UNSUPPORTED
+ * otherwise).  Entries sharing the same X and AX pointers are fused into one pass. */
+cqg_status cqg_twoe_contract_direct(cqg_ctx *ctx, int nmat, const double *const *X,
+                                    double *const *AX, const int *types, const double *scale,
+                                    int ld, int on_device, void *stream);
+
+/* SingleSlater<double>::formPT (include/singleslater/singleslater_fock.h:31-93): zeroes
+ * PTs (and PTz) and builds  RHF: PTs = 2J[Ps] + 2 xHF K[Ps]
+ *                           UHF: additionally PTz = 2 xHF K[Pz]
+ * (xHF = -0.5 for Hartree-Fock, include/singleslater.h:455).  Pz/PTz NULL for RHF. */
+cqg_status cqg_form_pt(cqg_ctx *ctx, int is_rhf, double xHF, const double *Ps,
+                       const double *Pz, double *PTs, double *PTz, int ld, int on_device,
+                       void *stream);
+
+/* Statistics of the last contraction (synchronises the context's stream). */
+cqg_status cqg_get_stats(cqg_ctx *ctx, cqg_stats *out);
+/* Per-class kernel timing on (1) / off (0, default). */
+cqg_status cqg_set_timing(cqg_ctx *ctx, int on);
+/* Name of quartet class index k ("(pp|ps)"), or NULL past the last class. */
+const char *cqg_class_name(int k);
+
+/* FP64 / FP32 FMA throughput probe used to report roofline fractions: runs a dependent
+ * FMA chain kernel for `ms_target` ms and returns achieved TFLOP/s in *tflops. */
+cqg_status cqg_probe_fma_peak(int device, int fp64, double ms_target, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CQGPU_H */
