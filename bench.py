@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""Fock-build throughput of the direct two-electron contraction on B200.
+
+Workload (default): RHF Fock build G[D] = 2J[D] - K[D] (``formPT``, reference
+include/singleslater/singleslater_fock.h:31-93 -> newTwoEContractDirect) for a seeded
+(H2O)_32 cluster at liquid density in cc-pVDZ (768 basis functions, quartet classes up to
+(dd|dd)), Schwarz threshold 1e-14 (the reference default, include/aointegrals.h:334).
+One step = one Fock build over one density.  Metric: screened unique shell quartets per
+second (the reference's loop unit, contract.h:96-131).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+The ``value`` leg times the device path (inputs resident in HBM, CUDA events on the
+launching stream, L2 flushed between steps).  ``e2e`` times the same build through the C
+ABI with host buffers (host->device and device->host copies inside the timed region).
+``--impl reference`` times the CPU restatement of the reference loop (the oracle; the
+reference itself needs Libint and cannot be built here) on the host cores, on a bounded
+slice of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "h2o32-ccpvdz": dict(nwater=32, basis="cc-pvdz", seed=1, thresh=1e-14),
+    "h2o8-ccpvdz": dict(nwater=8, basis="cc-pvdz", seed=1, thresh=1e-14),
+    "h2o1-631gd": dict(nwater=1, basis="6-31g*", seed=0, thresh=1e-12),
+}
+
+
+def synthetic_density(bs, seed):
+    """Seeded symmetric density with the distance decay of a molecular density matrix:
+    D_mn = u_mn exp(-0.5 R_mn) (+1 on the diagonal), u uniform in [-1, 1], R_mn the
+    distance in bohr between the centres of functions m and n."""
+    rng = np.random.default_rng(seed)
+    cent = np.concatenate([np.repeat(s.origin[None, :], s.size, axis=0) for s in bs.shells])
+    R = np.linalg.norm(cent[:, None, :] - cent[None, :, :], axis=-1)
+    u = rng.uniform(-1, 1, (bs.nbasis, bs.nbasis))
+    D = 0.5 * (u + u.T) * np.exp(-0.5 * R)
+    D[np.diag_indices_from(D)] += 1.0
+    return np.ascontiguousarray(D)
+
+
+def build_workload(name):
+    from chronusq_public_b200.basis import BasisSet
+    from chronusq_public_b200.molecule import water_cluster, single_water
+    w = WORKLOADS[name]
+    mol = single_water(w["seed"]) if w["nwater"] == 1 else water_cluster(w["nwater"], w["seed"])
+    bs = BasisSet(w["basis"], mol.atoms, mol.coords)
+    D = synthetic_density(bs, 1234)
+    return w, mol, bs, D
+
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.3)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, f[2:]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_baseline(bs, D, thresh, target_s=15.0, nthreads=0):
+    """Time the oracle (CPU restatement of the reference loop) on a bounded slice of the
+    same workload: all quartets whose largest shell index s1 lies in a window at the top
+    of the shell range, grown until the slice takes about `target_s` seconds."""
+    from oracle import oracle as O
+    ob = O.OracleBasis.from_basis(bs)
+    Q = O.schwarz(ob)
+    Dm = np.asfortranarray(D)
+    nsh = bs.nshell
+    width = 1
+    threads = nthreads or os.cpu_count()
+    while True:
+        G = np.zeros_like(Dm, order="F")
+        t0 = time.perf_counter()
+        n = O.twoe_contract_direct(ob, [Dm, Dm], [G, G], [0, 1], [1.0, -0.5], thresh=thresh, Q=Q,
+                                   nthreads=threads, s1_range=(nsh - width, nsh))
+        dt = time.perf_counter() - t0
+        if dt >= target_s / 4 or width >= nsh:
+            scale = max(1, int(round(target_s / max(dt, 1e-3))))
+            if scale > 1 and width < nsh:
+                width = min(nsh, width * int(math.ceil(scale ** (1 / 3.0))))
+                G = np.zeros_like(Dm, order="F")
+                t0 = time.perf_counter()
+                n = O.twoe_contract_direct(ob, [Dm, Dm], [G, G], [0, 1], [1.0, -0.5], thresh=thresh, Q=Q,
+                                           nthreads=threads, s1_range=(nsh - width, nsh))
+                dt = time.perf_counter() - t0
+            return {"value": n / dt, "unit": "quartets/s", "cores": threads, "kind": "port",
+                    "sample": "oracle restatement of newTwoEContractDirect (FP64 Obara-Saika/HGP, OpenMP), "
+                              "quartets with s1 in [%d,%d) of %d shells: %d quartets in %.2f s"
+                              % (nsh - width, nsh, nsh, n, dt),
+                    "quartets": n, "seconds": dt}
+        width *= 2
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    w, mol, bs, D = build_workload(args.workload)
+    base = cpu_baseline(bs, D, w["thresh"], target_s=args.ref_seconds)
+    from oracle import oracle as O
+    ob = O.OracleBasis.from_basis(bs)
+    Q = O.schwarz(ob)
+    nsh = bs.nshell
+    width = int(base["sample"].split("[")[1].split(",")[0])
+    lo = width
+    times, counts = [], []
+    Dm = np.asfortranarray(D)
+    for it in range(args.warmup + args.steps):
+        G = np.zeros_like(Dm, order="F")
+        t0 = time.perf_counter()
+        n = O.twoe_contract_direct(ob, [Dm, Dm], [G, G], [0, 1], [1.0, -0.5], thresh=w["thresh"], Q=Q,
+                                   nthreads=os.cpu_count(), s1_range=(lo, nsh))
+        dt = time.perf_counter() - t0
+        if it >= args.warmup:
+            times.append(dt)
+            counts.append(n)
+    v = sum(counts) / sum(times)
+    line = {"impl": "reference", "metric": "fock_build_quartets_per_s", "value": v, "unit": "quartets/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_of(args, w, bs),
+            "cpu_baseline": {"value": v, "unit": "quartets/s", "cores": os.cpu_count(), "kind": "port",
+                             "sample": "each step: oracle restatement (no Libint here) on quartets with s1 in "
+                                       "[%d,%d) of %d shells (%d quartets)" % (lo, nsh, nsh, counts[0])},
+            "e2e": {"value": v, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def config_of(args, w, bs):
+    return {"workload": args.workload, "molecule": "(H2O)_%d" % w["nwater"], "basis": w["basis"],
+            "nbasis": bs.nbasis, "nshell": bs.nshell, "schwarz_threshold": w["thresh"],
+            "density": "seeded synthetic, distance-decaying", "l2": "flushed between steps (256 MiB write)",
+            "precision": "fp64", "parallelism": "replicas" if args.gpus > 1 else "single"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="h2o32-ccpvdz", choices=sorted(WORKLOADS))
+    ap.add_argument("--ref-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--class-table", action="store_true", help="print per-class times to stderr")
+    args = ap.parse_args()
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        return run_reference(args, ws, rank)
+
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        pg = dist
+    from chronusq_public_b200.aointegrals import AOIntegrals, probe_fma_peak
+    from chronusq_public_b200 import _lib
+
+    w, mol, bs, D = build_workload(args.workload)
+    n = bs.nbasis
+    ints = AOIntegrals(bs, device=local, thresholdSchwartz=w["thresh"])
+    Dd = torch.from_numpy(D).cuda()
+    PT = torch.zeros_like(Dd)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    for _ in range(args.warmup):
+        ints.formPT(Dd, PTs=PT)
+    torch.cuda.synchronize()
+    ints.setTiming(True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    step_ms, eri_ms, quartets, mflops, launches, class_ms = [], [], [], [], 0, {}
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            ints.formPT(Dd, PTs=PT)
+            ev[k][1].record(stream)
+            st = ints.stats()
+            quartets.append(st["quartets"])
+            mflops.append(st["model_flops"])
+            eri_ms.append(st["ms_eri"])
+            launches += st["launches"]
+            for c, v in st["class_ms"].items():
+                class_ms[c] = class_ms.get(c, 0.0) + v / args.steps
+        torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    ints.setTiming(False)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    tot_ms = sum(step_ms)
+    if pg:
+        t = torch.tensor([tot_ms], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        tot_ms = float(t.item())
+    value = ws * sum(quartets) / (tot_ms * 1e-3)
+    st_last = ints.stats()
+
+    # end to end through the C ABI with pinned host buffers
+    Dh = torch.from_numpy(D).pin_memory()
+    PTh = torch.zeros_like(Dh).pin_memory()
+    L = _lib.lib()
+    e2e_t = []
+    for k in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rc = L.cqg_form_pt(ints._ctx, 1, -0.5, ctypes.c_void_p(Dh.data_ptr()), None,
+                           ctypes.c_void_p(PTh.data_ptr()), None, n, 0, ctypes.c_void_p(stream.cuda_stream))
+        _lib.check(rc, ints._ctx)
+        t1 = time.perf_counter()
+        if k >= args.warmup:
+            e2e_t.append(t1 - t0)
+    e2e_val = ws * quartets[0] / (sum(e2e_t) / len(e2e_t))
+    if pg:
+        t = torch.tensor([sum(e2e_t)], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_val = ws * quartets[0] * len(e2e_t) / float(t.item())
+    err = float(np.abs(PTh.numpy() - PT.cpu().numpy()).max())
+
+    if rank == 0:
+        peak64 = probe_fma_peak(True, 100.0, local)
+        eri_s = sum(eri_ms) / len(eri_ms) * 1e-3
+        achieved = (sum(mflops) / len(mflops)) / eri_s / 1e12
+        traffic = None
+        tj = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tj):
+            try:
+                tr = json.load(open(tj)).get(args.workload)
+                if tr:
+                    traffic = tr["bytes_per_quartet"] * quartets[0]
+            except (ValueError, KeyError):
+                traffic = None
+        line = {
+            "metric": "fock_build_quartets_per_s", "value": value, "unit": "quartets/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config_of(args, w, bs),
+            "quartets_per_step": quartets[0], "fock_builds_per_s": 1e3 * args.steps / tot_ms,
+            "e2e": {"value": e2e_val, "unit": "quartets/s", "h2d_bytes_per_step": 2 * n * n * 8,
+                    "d2h_bytes_per_step": n * n * 8, "max_abs_diff_vs_device_path": err},
+            "roofline": {"bound": "fp64", "kernel": "k_eri_jk (all quartet classes, ERI + J/K digest)",
+                         "achieved": achieved, "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64,
+                         "peak_source": "measured: FP64 FMA-chain probe (cqg_probe_fma_peak) on this GPU",
+                         "flop_model": "MD-v1 (model FLOPs of the screened quartets)",
+                         "model_flops_per_step": mflops[0], "eri_ms_per_step": eri_s * 1e3,
+                         "traffic": traffic},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        if not args.no_cpu_baseline and ws == 1:
+            line["cpu_baseline"] = cpu_baseline(bs, D, w["thresh"], target_s=args.ref_seconds)
+        print(json.dumps(line), flush=True)
+        if args.class_table:
+            for c, v in sorted(class_ms.items(), key=lambda kv: -kv[1]):
+                if v > 0:
+                    print("%-8s %9.3f ms  %12d quartets" % (c, v, st_last["class_quartets"][c]), file=sys.stderr)
+    ints.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

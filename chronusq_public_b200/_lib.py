@@ -42,6 +42,7 @@ class CqgStats(ctypes.Structure):
         ("ms_screen", ctypes.c_double),
         ("ms_eri", ctypes.c_double),
         ("ms_total", ctypes.c_double),
+        ("launches", ctypes.c_longlong),
         ("class_quartets", ctypes.c_longlong * 55),
         ("class_ms", ctypes.c_double * 55),
     ]

@@ -130,6 +130,7 @@ class AOIntegrals:
             "quartets": int(s.quartets), "quartets_fp32": int(s.quartets_fp32),
             "prim_quartets": int(s.prim_quartets), "model_flops": float(s.model_flops),
             "ms_screen": s.ms_screen, "ms_eri": s.ms_eri, "ms_total": s.ms_total,
+            "launches": int(s.launches),
             "class_quartets": {names[k]: int(s.class_quartets[k]) for k in range(len(names))},
             "class_ms": {names[k]: float(s.class_ms[k]) for k in range(len(names))},
         }

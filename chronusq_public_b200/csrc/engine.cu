@@ -26,11 +26,13 @@
 #include "../../include/cqgpu.h"
 #include "eri_common.cuh"
 #include "_gen/eri_classes.cuh"
+#include "eri_warp.cuh"
 
 #define CQG_MAXL 2
 #define CQG_NPC ((CQG_MAXL + 1) * (CQG_MAXL + 2) / 2)       // pair classes
 #define CQG_NQC (CQG_NPC * (CQG_NPC + 1) / 2)                // quartet classes
 #define CQG_MAXG 4
+#define CQG_NBUCKET 8
 
 static_assert(CQG_NQC <= 55, "class table");
 
@@ -76,7 +78,8 @@ struct Pairs {
   const int2 *sh;       // (shell a, shell b), internal orientation L_a >= L_b
   const double *Q;      // Schwarz bound
   const int *poff;      // first primitive pair
-  const int *np;        // number of primitive pairs
+  const int *np;        // number of primitive pairs (after primitive screening)
+  const int *kk;        // nprim(a) * nprim(b) of the contracted shells (model count)
   const PrimPair *prim;
 };
 struct DigestGroups {
@@ -92,8 +95,11 @@ struct DigestGroups {
 // ------------------------------------------------------------------ kernels ---
 // Schwarz: Q(ab) = sqrt(max_ij |(ij|ij)|) for pairs [beg, end) of one class.
 template <int LA, int LB>
-__global__ void __launch_bounds__(128) k_schwarz(Pairs P, Shells S, const double *__restrict__ boys,
+__global__ void __launch_bounds__(128) k_schwarz(Pairs P, Shells S, const double *__restrict__ boys_g,
                                                  int beg, int end, double *__restrict__ Qout) {
+  __shared__ double boys[BOYS_NT * BOYS_SROW];
+  stage_boys<2 * (LA + LB)>(boys_g, boys);
+  __syncthreads();
   int i = beg + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= end) return;
   constexpr int NA = nfun_c(LA), NB = nfun_c(LB), NAB = NA * NB;
@@ -165,6 +171,7 @@ struct BlockTable {
   int ket_beg[CQG_NQC];        // first ket pair (global index) of the block
   int ket_n[CQG_NQC];          // number of ket pairs of the block's ket class
   int diag[CQG_NQC];           // bra class == ket class
+  int ket_bucket[CQG_NQC][CQG_NBUCKET + 1];  // global start of each primitive bucket of the ket class
 };
 
 __device__ __forceinline__ int find_block(const BlockTable &bt, int task) {
@@ -203,7 +210,7 @@ template <bool FILL>
 __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pairs P, const double *__restrict__ M,
                                                   int nsh, const double *__restrict__ Mmax, double thresh,
                                                   long long *__restrict__ cnt, const long long *__restrict__ off,
-                                                  uint2 *__restrict__ qlist) {
+                                                  uint2 *__restrict__ qlist, unsigned long long *__restrict__ blkacc) {
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (warp >= ntask) return;
@@ -211,29 +218,47 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
   int bra = bt.bra_beg[blk] + (warp - bt.task_beg[blk]);
   double qb = P.Q[bra];
   double mm = *Mmax;
-  int kn = bt.ket_n[blk];
-  int nk = 0;
-  if (qb * mm > 0.0) {
-    double cut = thresh / (qb * mm) * (1.0 - 1e-12);
-    nk = coarse_range(P.Q, bt.ket_beg[blk], kn, cut);
-  }
-  if (bt.diag[blk]) nk = min(nk, bra - bt.bra_beg[blk] + 1);
+  double cut = (qb * mm > 0.0) ? thresh / (qb * mm) * (1.0 - 1e-12) : 0.0;
   int2 ab = P.sh[bra];
   long long base = FILL ? off[warp] : 0;
   long long c = 0;
-  for (int k0 = 0; k0 < nk; k0 += 32) {
-    int k = k0 + lane;
-    bool pass = false;
-    int ket = bt.ket_beg[blk] + k;
-    if (k < nk) pass = exact_pass(M, nsh, ab, P.sh[ket], qb, P.Q[ket], thresh);
-    unsigned bal = __ballot_sync(0xffffffffu, pass);
-    if (FILL && pass) {
-      int pos = __popc(bal & ((1u << lane) - 1u));
-      qlist[base + c + pos] = make_uint2((unsigned)bra, (unsigned)ket);
+  unsigned long long kmodel = 0, kexec = 0;
+  if (qb * mm > 0.0) {
+    for (int bk = 0; bk < CQG_NBUCKET; ++bk) {
+      const int kb = bt.ket_bucket[blk][bk], ke = bt.ket_bucket[blk][bk + 1];
+      if (ke <= kb) continue;
+      int kend = kb + coarse_range(P.Q, kb, ke - kb, cut);
+      if (bt.diag[blk]) kend = min(kend, bra + 1);   // unique pairs of pairs: ket <= bra
+      for (int k0 = kb; k0 < kend; k0 += 32) {
+        int ket = k0 + lane;
+        bool pass = false;
+        if (ket < kend) pass = exact_pass(M, nsh, ab, P.sh[ket], qb, P.Q[ket], thresh);
+        unsigned bal = __ballot_sync(0xffffffffu, pass);
+        if (FILL && pass) {
+          int pos = __popc(bal & ((1u << lane) - 1u));
+          qlist[base + c + pos] = make_uint2((unsigned)bra, (unsigned)ket);
+        }
+        if (!FILL && pass) {
+          kmodel += (unsigned long long)P.kk[ket];
+          kexec += (unsigned long long)P.np[ket];
+        }
+        c += __popc(bal);
+      }
     }
-    c += __popc(bal);
   }
-  if (!FILL && lane == 0) cnt[warp] = c;
+  if (!FILL) {
+    for (int o = 16; o > 0; o >>= 1) {
+      kmodel += __shfl_xor_sync(0xffffffffu, kmodel, o);
+      kexec += __shfl_xor_sync(0xffffffffu, kexec, o);
+    }
+    if (lane == 0) {
+      cnt[warp] = c;
+      if (c) {
+        atomicAdd(blkacc + 2 * blk, kmodel * (unsigned long long)P.kk[bra]);
+        atomicAdd(blkacc + 2 * blk + 1, kexec * (unsigned long long)P.np[bra]);
+      }
+    }
+  }
 }
 
 // block ranges [beg, end) of the quartet list from the per-task counts and offsets
@@ -253,25 +278,40 @@ __global__ void k_block_ranges(BlockTable bt, const long long *__restrict__ cnt,
   range[2 * b + 1] = end;
 }
 
+__device__ __forceinline__ double warp_sum(double x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+// J/K digest of one quartet (contract.h:145-171), half of the updates:
+//   COULOMB : Gh(a,b) += sJ sum_cd X(d,c) v ;  Gh(c,d) += sJ sum_ab X(b,a) v
+//   EXCHANGE: Gh(a,c) += sK X(b,d) v ; Gh(b,d) += sK X(a,c) v ; Gh(a,d) += sK X(b,c) v ;
+//             Gh(b,c) += sK X(a,d) v
+// with v = (ab|cd) * degeneracy, sK = 0.5 * scale_K; the other half is Gh^T (added in
+// k_finalize).  All lanes of the warp call this; `valid` lanes hold a quartet, and when
+// every lane shares the bra pair (`bra_uniform`) the Gh(a,b) sums are reduced across the
+// warp before one atomic per element.
 template <int NA, int NB, int NC, int ND>
 __device__ __forceinline__ void digest(const double *v, double deg, int a0, int b0, int c0, int d0,
-                                       const DigestGroups &dg) {
+                                       const DigestGroups &dg, bool valid, bool bra_uniform) {
   const size_t ld = dg.ldx, n = dg.n;
+  const int lane = threadIdx.x & 31;
   for (int g = 0; g < dg.ng; ++g) {
     const double *__restrict__ X = dg.X[g];
     double *G = dg.G[g];
     const double sJ = dg.sJ[g] * deg;
     const double sK = 0.5 * dg.sK[g] * deg;
-    if (sJ != 0.0) {
+    if (dg.sJ[g] != 0.0) {
       double xdc[NC * ND], xba[NA * NB];
 #pragma unroll
       for (int c = 0; c < NC; ++c)
 #pragma unroll
-        for (int d = 0; d < ND; ++d) xdc[c * ND + d] = __ldg(X + (d0 + d) + (c0 + c) * ld);
+        for (int d = 0; d < ND; ++d) xdc[c * ND + d] = valid ? __ldg(X + (d0 + d) + (c0 + c) * ld) : 0.0;
 #pragma unroll
       for (int a = 0; a < NA; ++a)
 #pragma unroll
-        for (int b = 0; b < NB; ++b) xba[a * NB + b] = __ldg(X + (b0 + b) + (a0 + a) * ld);
+        for (int b = 0; b < NB; ++b) xba[a * NB + b] = valid ? __ldg(X + (b0 + b) + (a0 + a) * ld) : 0.0;
 #pragma unroll
       for (int a = 0; a < NA; ++a)
 #pragma unroll
@@ -279,18 +319,25 @@ __device__ __forceinline__ void digest(const double *v, double deg, int a0, int 
           double s = 0.0;
 #pragma unroll
           for (int cd = 0; cd < NC * ND; ++cd) s += xdc[cd] * v[(a * NB + b) * NC * ND + cd];
-          atomicAdd(G + (a0 + a) + (b0 + b) * n, sJ * s);
+          s *= sJ;
+          if (bra_uniform) {
+            s = warp_sum(s);
+            if (lane == 0) atomicAdd(G + (a0 + a) + (b0 + b) * n, s);
+          } else if (valid) {
+            atomicAdd(G + (a0 + a) + (b0 + b) * n, s);
+          }
         }
+      if (valid) {
 #pragma unroll
-      for (int cd = 0; cd < NC * ND; ++cd) {
-        double s = 0.0;
+        for (int cd = 0; cd < NC * ND; ++cd) {
+          double s = 0.0;
 #pragma unroll
-        for (int ab = 0; ab < NA * NB; ++ab) s += xba[ab] * v[ab * NC * ND + cd];
-        atomicAdd(G + (c0 + cd / ND) + (d0 + cd % ND) * n, sJ * s);
+          for (int ab = 0; ab < NA * NB; ++ab) s += xba[ab] * v[ab * NC * ND + cd];
+          atomicAdd(G + (c0 + cd / ND) + (d0 + cd % ND) * n, sJ * s);
+        }
       }
     }
-    if (sK != 0.0) {
-      // G(a,c) += X(b,d) v ; G(b,d) += X(a,c) v ; G(a,d) += X(b,c) v ; G(b,c) += X(a,d) v
+    if (dg.sK[g] != 0.0 && valid) {
       double xbd[NB * ND], xac[NA * NC], xbc[NB * NC], xad[NA * ND];
 #pragma unroll
       for (int b = 0; b < NB; ++b)
@@ -357,21 +404,325 @@ __device__ __forceinline__ void digest(const double *v, double deg, int a0, int 
 }
 
 template <int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void eri_jk_one(const uint2 *__restrict__ ql, long long i, long long wfirst, long long end,
+                                           const Pairs &P, const Shells &S, const double *boys,
+                                           const DigestGroups &dg);
+
+// Per-thread class kernel: persistent grid over the class's quartet range; the Boys rows
+// of this class are staged in shared memory once per block.
+template <int LA, int LB, int LC, int LD>
 __global__ void __launch_bounds__(128) k_eri_jk(const uint2 *__restrict__ ql, const long long *__restrict__ range,
-                                                int blk, Pairs P, Shells S, const double *__restrict__ boys,
+                                                int blk, Pairs P, Shells S, const double *__restrict__ boys_g,
                                                 DigestGroups dg) {
+  __shared__ double boys[BOYS_NT * BOYS_SROW];
+  stage_boys<LA + LB + LC + LD>(boys_g, boys);
+  __syncthreads();
   const long long beg = range[2 * blk], end = range[2 * blk + 1];
-  const long long i = beg + blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= end) return;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = beg + blockIdx.x * (long long)blockDim.x + threadIdx.x;; i += stride) {
+    const long long wfirst = i - (threadIdx.x & 31);
+    if (wfirst >= end) return;   // the whole warp is past the end of the class
+    eri_jk_one<LA, LB, LC, LD>(ql, i, wfirst, end, P, S, boys, dg);
+  }
+}
+
+template <int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void eri_jk_one(const uint2 *__restrict__ ql, long long i, long long wfirst, long long end,
+                                           const Pairs &P, const Shells &S, const double *boys,
+                                           const DigestGroups &dg) {
+  const bool valid = i < end;
   constexpr int NA = nfun_c(LA), NB = nfun_c(LB), NC = nfun_c(LC), ND = nfun_c(LD);
-  const uint2 e = ql[i];
+  const uint2 e = ql[valid ? i : wfirst];
   const int2 ab = P.sh[e.x], cd = P.sh[e.y];
-  const double3 A = S.center[ab.x], B = S.center[ab.y], C = S.center[cd.x], D = S.center[cd.y];
   double v[NA * NB * NC * ND];
-  EriClass<LA, LB, LC, LD>::template run<double>(P.prim + P.poff[e.x], P.np[e.x], P.prim + P.poff[e.y],
-                                                 P.np[e.y], A, B, C, D, boys, v);
+  if (valid) {
+    const double3 A = S.center[ab.x], B = S.center[ab.y], C = S.center[cd.x], D = S.center[cd.y];
+    EriClass<LA, LB, LC, LD>::template run<double>(P.prim + P.poff[e.x], P.np[e.x], P.prim + P.poff[e.y],
+                                                   P.np[e.y], A, B, C, D, boys, v);
+  } else {
+#pragma unroll
+    for (int k = 0; k < NA * NB * NC * ND; ++k) v[k] = 0.0;
+  }
+  const unsigned bra0 = __shfl_sync(0xffffffffu, e.x, 0);
+  const bool uniform = __all_sync(0xffffffffu, e.x == bra0);
   const double deg = (ab.x == ab.y ? 1.0 : 2.0) * (cd.x == cd.y ? 1.0 : 2.0) * (e.x == e.y ? 1.0 : 2.0);
-  digest<NA, NB, NC, ND>(v, deg, S.bf[ab.x], S.bf[ab.y], S.bf[cd.x], S.bf[cd.y], dg);
+  digest<NA, NB, NC, ND>(v, deg, S.bf[ab.x], S.bf[ab.y], S.bf[cd.x], S.bf[cd.y], dg, valid, uniform);
+}
+
+// ------------------------------------------------------------- warp-mode classes ---
+// SCHWARZ = false: quartets from the list, J/K digest.  SCHWARZ = true: "quartet" i is
+// pair i with itself, and the kernel writes Q(i) = sqrt(max |(ab|ab)| diagonal).
+template <int LA, int LB, int LC, int LD, bool SCHWARZ>
+__global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ ql, const long long *__restrict__ range,
+                                                     int blk, long long sbeg, long long send, Pairs P, Shells S,
+                                                     const double *__restrict__ boys, DigestGroups dg,
+                                                     double *__restrict__ Qout) {
+  using WD = warpmd::WarpDims<LA, LB, LC, LD>;
+  constexpr int L = WD::L, NCCD = WD::NCCD;
+  constexpr int NBUF = (WD::NW > WD::NC) ? WD::NW : WD::NC;
+  extern __shared__ double smem[];
+  // decode tables: Hermite (t,u,v) of index h, and Cartesian exponents of bra / ket pairs,
+  // packed 4 bits per exponent
+  __shared__ int s_h[WD::HL];
+  __shared__ int s_cab[WD::NCAB];
+  __shared__ int s_ccd[NCCD];
+  for (int k = threadIdx.x; k < WD::HL; k += blockDim.x) {
+    int t, u, v;
+    warpmd::herm_of(k, t, u, v);
+    s_h[k] = t | (u << 4) | (v << 8);
+  }
+  for (int k = threadIdx.x; k < WD::NCAB; k += blockDim.x) {
+    int x0, y0, z0, x1, y1, z1;
+    warpmd::cart_of(LA, k / warpmd::ncart(LB), x0, y0, z0);
+    warpmd::cart_of(LB, k % warpmd::ncart(LB), x1, y1, z1);
+    s_cab[k] = x0 | (y0 << 4) | (z0 << 8) | (x1 << 12) | (y1 << 16) | (z1 << 20);
+  }
+  for (int k = threadIdx.x; k < NCCD; k += blockDim.x) {
+    int x0, y0, z0, x1, y1, z1;
+    warpmd::cart_of(LC, k / warpmd::ncart(LD), x0, y0, z0);
+    warpmd::cart_of(LD, k % warpmd::ncart(LD), x1, y1, z1);
+    s_ccd[k] = x0 | (y0 << 4) | (z0 << 8) | (x1 << 12) | (y1 << 16) | (z1 << 20);
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double *Eb = smem + (size_t)wid * (3 * WD::NEB + 3 * WD::NEK + 2 * WD::HL + 2 * NBUF + WD::NXS);
+  double *Ek = Eb + 3 * WD::NEB;
+  double *Ra = Ek + 3 * WD::NEK;
+  double *Rb = Ra + WD::HL;
+  double *W = Rb + WD::HL;
+  double *Cc = W + NBUF;
+  double *Xs = Cc + NBUF;   // staged density blocks for the digest
+  long long beg, end;
+  if (SCHWARZ) {
+    beg = sbeg;
+    end = send;
+  } else {
+    beg = range[2 * blk];
+    end = range[2 * blk + 1];
+  }
+  const long long stride = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long q = beg + (long long)blockIdx.x * (blockDim.x >> 5) + wid; q < end; q += stride) {
+    uint2 e;
+    if (SCHWARZ) e = make_uint2((unsigned)q, (unsigned)q);
+    else e = ql[q];
+    const int2 ab = P.sh[e.x], cdp = P.sh[e.y];
+    const double3 A = S.center[ab.x], B = S.center[ab.y], C = S.center[cdp.x], D = S.center[cdp.y];
+    const PrimPair *pbp = P.prim + P.poff[e.x];
+    const PrimPair *pkp = P.prim + P.poff[e.y];
+    const int nb = P.np[e.x], nk = P.np[e.y];
+    __syncwarp();
+    for (int k = lane; k < WD::NC; k += 32) Cc[k] = 0.0;
+    for (int ib = 0; ib < nb; ++ib) {
+      const PrimPair bp = pbp[ib];
+      __syncwarp();
+      if (lane < 3) {
+        const double Pc = lane == 0 ? bp.Px : (lane == 1 ? bp.Py : bp.Pz);
+        const double Ac = lane == 0 ? A.x : (lane == 1 ? A.y : A.z);
+        const double Bc = lane == 0 ? B.x : (lane == 1 ? B.y : B.z);
+        warpmd::build_E1<LA, LB, double>(Eb + lane * WD::NEB, Pc - Ac, Pc - Bc, 0.5 * bp.ip);
+      }
+      for (int k = lane; k < WD::NW; k += 32) W[k] = 0.0;
+      for (int ik = 0; ik < nk; ++ik) {
+        const PrimPair kp = pkp[ik];
+        __syncwarp();
+        if (lane < 3) {
+          const double Pc = lane == 0 ? kp.Px : (lane == 1 ? kp.Py : kp.Pz);
+          const double Cc3 = lane == 0 ? C.x : (lane == 1 ? C.y : C.z);
+          const double Dc = lane == 0 ? D.x : (lane == 1 ? D.y : D.z);
+          warpmd::build_E1<LC, LD, double>(Ek + lane * WD::NEK, Pc - Cc3, Pc - Dc, 0.5 * kp.ip);
+        }
+        const double pq = bp.p + kp.p;
+        const double rpq = rsqrt(pq);
+        const double rho = bp.p * kp.p * (rpq * rpq);
+        const double X = bp.Px - kp.Px, Y = bp.Py - kp.Py, Z = bp.Pz - kp.Pz;
+        double F[L + 1];
+        boys_eval<L>(rho * (X * X + Y * Y + Z * Z), boys, F);
+        double fac[L + 1];
+        {
+          double f = bp.Kp * kp.Kp * rpq;
+          const double m2r = -2.0 * rho;
+#pragma unroll
+          for (int n = 0; n <= L; ++n) {
+            fac[n] = f * F[n];
+            f *= m2r;
+          }
+        }
+        // R^{(n)}_{tuv}, n = L .. 0, ping-pong between Ra and Rb; level L in Ra when L even
+        double *prev = (L % 2 == 0) ? Rb : Ra;
+        double *cur = (L % 2 == 0) ? Ra : Rb;
+        // level L: one entry
+        if (lane == 0) cur[0] = fac[L];
+#pragma unroll 1
+        for (int n = L - 1; n >= 0; --n) {
+          double *t_ = prev;
+          prev = cur;
+          cur = t_;
+          __syncwarp();
+          const int cnt = warpmd::nherm(L - n);
+          for (int h = lane; h < cnt; h += 32) {
+            double val;
+            if (h == 0) {
+              val = fac[n];
+            } else {
+              const int hc = s_h[h];
+              const int t = hc & 15, u = (hc >> 4) & 15, v = hc >> 8;
+              if (t > 0) {
+                val = X * prev[warpmd::hidx(t - 1, u, v)];
+                if (t > 1) val += (t - 1) * prev[warpmd::hidx(t - 2, u, v)];
+              } else if (u > 0) {
+                val = Y * prev[warpmd::hidx(t, u - 1, v)];
+                if (u > 1) val += (u - 1) * prev[warpmd::hidx(t, u - 2, v)];
+              } else {
+                val = Z * prev[warpmd::hidx(t, u, v - 1)];
+                if (v > 1) val += (v - 1) * prev[warpmd::hidx(t, u, v - 2)];
+              }
+            }
+            cur[h] = val;
+          }
+        }
+        __syncwarp();
+        const double *R = cur;  // level 0
+        // W[tuv][cd] += sum (-1)^(tau+nu+phi) E^cd R
+        for (int e2 = lane; e2 < WD::NW; e2 += 32) {
+          const int h = e2 / NCCD, c = e2 % NCCD;
+          const int hc = s_h[h], cc = s_ccd[c];
+          const int t = hc & 15, u = (hc >> 4) & 15, v = hc >> 8;
+          const int cx = cc & 15, cy = (cc >> 4) & 15, cz = (cc >> 8) & 15;
+          const int dx = (cc >> 12) & 15, dy = (cc >> 16) & 15, dz = cc >> 20;
+          constexpr int NT = WD::Q + 1;
+          const double *ex = Ek + (cx * (LD + 1) + dx) * NT;
+          const double *ey = Ek + WD::NEK + (cy * (LD + 1) + dy) * NT;
+          const double *ez = Ek + 2 * WD::NEK + (cz * (LD + 1) + dz) * NT;
+          double s = 0.0;
+          for (int a1 = 0; a1 <= cx + dx; ++a1)
+            for (int a2 = 0; a2 <= cy + dy; ++a2) {
+              const double exy = ((a1 + a2) & 1 ? -1.0 : 1.0) * ex[a1] * ey[a2];
+              for (int a3 = 0; a3 <= cz + dz; ++a3) {
+                const double c3 = (a3 & 1) ? -ez[a3] : ez[a3];
+                s += exy * c3 * R[warpmd::hidx(t + a1, u + a2, v + a3)];
+              }
+            }
+          W[e2] += s;
+        }
+      }
+      __syncwarp();
+      // C[ab][cd] += sum_tuv E^ab_tuv W[tuv][cd]
+      for (int e2 = lane; e2 < WD::NC; e2 += 32) {
+        const int abi = e2 / NCCD, c = e2 % NCCD;
+        const int cc = s_cab[abi];
+        const int ax = cc & 15, ay = (cc >> 4) & 15, az = (cc >> 8) & 15;
+        const int bx = (cc >> 12) & 15, by = (cc >> 16) & 15, bz = cc >> 20;
+        constexpr int NT = WD::P + 1;
+        const double *ex = Eb + (ax * (LB + 1) + bx) * NT;
+        const double *ey = Eb + WD::NEB + (ay * (LB + 1) + by) * NT;
+        const double *ez = Eb + 2 * WD::NEB + (az * (LB + 1) + bz) * NT;
+        double s = 0.0;
+        for (int a1 = 0; a1 <= ax + bx; ++a1)
+          for (int a2 = 0; a2 <= ay + by; ++a2) {
+            const double exy = ex[a1] * ey[a2];
+            for (int a3 = 0; a3 <= az + bz; ++a3) s += exy * ez[a3] * W[warpmd::hidx(a1, a2, a3) * NCCD + c];
+          }
+        Cc[e2] += s;
+      }
+    }
+    __syncwarp();
+    // Cartesian -> spherical on pure axes (L > 1), ping-pong Cc <-> W
+    double *src = Cc, *dst = W;
+    {
+      int d[4] = {warpmd::ncart(LA), warpmd::ncart(LB), warpmd::ncart(LC), warpmd::ncart(LD)};
+      const int ls[4] = {LA, LB, LC, LD};
+#pragma unroll
+      for (int ax = 0; ax < 4; ++ax) {
+        if (ls[ax] < 2) continue;
+        const double *Ct = ls[ax] == 2 ? kSph2 : kSph3;
+        warpmd::sph_axis<double>(src, dst, d, ax, ls[ax], Ct, lane);
+        d[ax] = 2 * ls[ax] + 1;
+        double *t_ = src;
+        src = dst;
+        dst = t_;
+        __syncwarp();
+      }
+    }
+    const double *V = src;   // [a][b][c][d] in the reference basis
+    constexpr int NA = WD::NSA, NB = WD::NSB, NC = WD::NSC, ND = WD::NSD;
+    if (SCHWARZ) {
+      double mx = 0.0;
+      for (int k = lane; k < NA * NB; k += 32) mx = fmax(mx, fabs(V[k * (NA * NB) + k]));
+      for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      if (lane == 0) Qout[q] = sqrt(mx);
+      continue;
+    }
+    const double deg = (ab.x == ab.y ? 1.0 : 2.0) * (cdp.x == cdp.y ? 1.0 : 2.0) * (e.x == e.y ? 1.0 : 2.0);
+    const int a0 = S.bf[ab.x], b0 = S.bf[ab.y], c0 = S.bf[cdp.x], d0 = S.bf[cdp.y];
+    const size_t ld = dg.ldx, n = dg.n;
+    // staged blocks: X(d,c) [NC*ND], X(b,a) [NA*NB], X(b,d), X(a,c), X(b,c), X(a,d)
+    double *xdc = Xs, *xba = xdc + NC * ND, *xbd = xba + NA * NB, *xac = xbd + NB * ND;
+    double *xbc = xac + NA * NC, *xad = xbc + NB * NC;
+    for (int g = 0; g < dg.ng; ++g) {
+      const double *__restrict__ Xm = dg.X[g];
+      double *G = dg.G[g];
+      const double sJ = dg.sJ[g] * deg, sK = 0.5 * dg.sK[g] * deg;
+      __syncwarp();
+      for (int k = lane; k < NC * ND; k += 32) xdc[k] = __ldg(Xm + (d0 + k % ND) + (c0 + k / ND) * ld);
+      for (int k = lane; k < NA * NB; k += 32) xba[k] = __ldg(Xm + (b0 + k % NB) + (a0 + k / NB) * ld);
+      for (int k = lane; k < NB * ND; k += 32) xbd[k] = __ldg(Xm + (b0 + k / ND) + (d0 + k % ND) * ld);
+      for (int k = lane; k < NA * NC; k += 32) xac[k] = __ldg(Xm + (a0 + k / NC) + (c0 + k % NC) * ld);
+      for (int k = lane; k < NB * NC; k += 32) xbc[k] = __ldg(Xm + (b0 + k / NC) + (c0 + k % NC) * ld);
+      for (int k = lane; k < NA * ND; k += 32) xad[k] = __ldg(Xm + (a0 + k / ND) + (d0 + k % ND) * ld);
+      __syncwarp();
+      if (dg.sJ[g] != 0.0) {
+        for (int k = lane; k < NA * NB; k += 32) {
+          const int a = k / NB, b = k % NB;
+          double s = 0.0;
+          for (int cd = 0; cd < NC * ND; ++cd) s += xdc[cd] * V[k * NC * ND + cd];
+          atomicAdd(G + (a0 + a) + (b0 + b) * n, sJ * s);
+        }
+        for (int k = lane; k < NC * ND; k += 32) {
+          const int c = k / ND, d = k % ND;
+          double s = 0.0;
+          for (int ab2 = 0; ab2 < NA * NB; ++ab2) s += xba[ab2] * V[ab2 * NC * ND + k];
+          atomicAdd(G + (c0 + c) + (d0 + d) * n, sJ * s);
+        }
+      }
+      if (dg.sK[g] != 0.0) {
+        for (int k = lane; k < NA * NC; k += 32) {   // G(a,c) += X(b,d) v
+          const int a = k / NC, c = k % NC;
+          double s = 0.0;
+          for (int b = 0; b < NB; ++b)
+            for (int d = 0; d < ND; ++d) s += xbd[b * ND + d] * V[((a * NB + b) * NC + c) * ND + d];
+          atomicAdd(G + (a0 + a) + (c0 + c) * n, sK * s);
+        }
+        for (int k = lane; k < NB * ND; k += 32) {   // G(b,d) += X(a,c) v
+          const int b = k / ND, d = k % ND;
+          double s = 0.0;
+          for (int a = 0; a < NA; ++a)
+            for (int c = 0; c < NC; ++c) s += xac[a * NC + c] * V[((a * NB + b) * NC + c) * ND + d];
+          atomicAdd(G + (b0 + b) + (d0 + d) * n, sK * s);
+        }
+        for (int k = lane; k < NA * ND; k += 32) {   // G(a,d) += X(b,c) v
+          const int a = k / ND, d = k % ND;
+          double s = 0.0;
+          for (int b = 0; b < NB; ++b)
+            for (int c = 0; c < NC; ++c) s += xbc[b * NC + c] * V[((a * NB + b) * NC + c) * ND + d];
+          atomicAdd(G + (a0 + a) + (d0 + d) * n, sK * s);
+        }
+        for (int k = lane; k < NB * NC; k += 32) {   // G(b,c) += X(a,d) v
+          const int b = k / NC, c = k % NC;
+          double s = 0.0;
+          for (int a = 0; a < NA; ++a)
+            for (int d = 0; d < ND; ++d) s += xad[a * ND + d] * V[((a * NB + b) * NC + c) * ND + d];
+          atomicAdd(G + (b0 + b) + (c0 + c) * n, sK * s);
+        }
+      }
+    }
+  }
+}
+
+template <int LA, int LB, int LC, int LD>
+static size_t warp_smem_bytes() {
+  using WD = warpmd::WarpDims<LA, LB, LC, LD>;
+  constexpr int NBUF = (WD::NW > WD::NC) ? WD::NW : WD::NC;
+  return sizeof(double) * 4 * (size_t)(3 * WD::NEB + 3 * WD::NEK + 2 * WD::HL + 2 * NBUF + WD::NXS);
 }
 
 // AX += 0.5 (Gh + Gh^T)
@@ -457,13 +808,16 @@ struct cqg_ctx {
   std::vector<double> Qmat;  // nshell x nshell
   // pairs, by class
   int pc_beg[CQG_NPC + 1] = {0};
+  int bucket_beg[CQG_NPC][CQG_NBUCKET + 1];
   std::vector<int2> pair_sh;
   std::vector<double> pair_Q;
   DevBuf<double3> d_center;
   DevBuf<int> d_bf, d_sz;
   DevBuf<int2> d_pair_sh;
   DevBuf<double> d_pair_Q;
-  DevBuf<int> d_pair_poff, d_pair_np;
+  DevBuf<int> d_pair_poff, d_pair_np, d_pair_kk;
+  DevBuf<unsigned long long> d_blkacc;
+  int launches = 0;
   DevBuf<PrimPair> d_prim;
   DevBuf<double> d_boys;
   long long prim_pairs_total = 0;
@@ -499,12 +853,45 @@ static double host_boys_row(int nmax, long double T, double *F) {
   return 0;
 }
 
+static Pairs make_pairs(cqg_ctx *ctx);
+static Shells make_shells(cqg_ctx *ctx);
+
+// classes evaluated by the warp-cooperative kernel (same rule as gen_eri.WARP_CLASSES)
+__host__ __device__ constexpr bool is_warp_class(int la, int lb, int lc, int ld) {
+  return ncart_c(la) * ncart_c(lb) * ncart_c(lc) * ncart_c(ld) > 150;
+}
+
+template <int LA, int LB, int LC, int LD, bool SCHWARZ>
+static cudaError_t launch_warp(cqg_ctx *ctx, int blk, long long n, long long sbeg, long long send, cudaStream_t st,
+                               const DigestGroups &dg, double *Q) {
+  if (n <= 0) return cudaSuccess;
+  static bool attr_set = false;
+  const size_t smem = warp_smem_bytes<LA, LB, LC, LD>();
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(k_eri_jk_warp<LA, LB, LC, LD, SCHWARZ>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  const int blocks = (int)std::min<long long>((n + 3) / 4, 148LL * 16);
+  k_eri_jk_warp<LA, LB, LC, LD, SCHWARZ><<<blocks, 128, smem, st>>>(ctx->d_qlist.p, ctx->d_range.p, blk, sbeg, send,
+                                                                    make_pairs(ctx), make_shells(ctx), ctx->d_boys.p,
+                                                                    dg, Q);
+  return cudaGetLastError();
+}
+
 template <int LA, int LB>
 static cudaError_t launch_schwarz(cqg_ctx *ctx, Pairs P, Shells S, int beg, int end, double *Q) {
   int n = end - beg;
   if (n <= 0) return cudaSuccess;
-  k_schwarz<LA, LB><<<(n + 127) / 128, 128>>>(P, S, ctx->d_boys.p, beg, end, Q);
-  return cudaGetLastError();
+  if constexpr (is_warp_class(LA, LB, LA, LB)) {
+    DigestGroups dg;
+    memset(&dg, 0, sizeof(dg));
+    return launch_warp<LA, LB, LA, LB, true>(ctx, 0, n, beg, end, 0, dg, Q);
+  } else {
+    k_schwarz<LA, LB><<<(n + 127) / 128, 128>>>(P, S, ctx->d_boys.p, beg, end, Q);
+    return cudaGetLastError();
+  }
 }
 
 static Pairs make_pairs(cqg_ctx *ctx) {
@@ -513,6 +900,7 @@ static Pairs make_pairs(cqg_ctx *ctx) {
   P.Q = ctx->d_pair_Q.p;
   P.poff = ctx->d_pair_poff.p;
   P.np = ctx->d_pair_np.p;
+  P.kk = ctx->d_pair_kk.p;
   P.prim = ctx->d_prim.p;
   return P;
 }
@@ -523,47 +911,66 @@ static Shells make_shells(cqg_ctx *ctx) {
   return S;
 }
 
-// build primitive-pair data for the current pair ordering; prim_thresh = 0 keeps all
+// Primitive pairs of shell pair (a, b); prim_thresh = 0 keeps all of them, otherwise a
+// pair whose s-type bound sqrt((ij|ij)) (with a (1+|AB|)^(la+lb) allowance) is below
+// prim_thresh is dropped.
+static void pair_prims(const cqg_ctx *ctx, int a, int b, double prim_thresh, std::vector<PrimPair> &out) {
+  const double pi = 3.14159265358979323846;
+  const double s2pi52 = std::sqrt(2.0 * std::pow(pi, 2.5));
+  const double *A = &ctx->hcent[3 * a], *B = &ctx->hcent[3 * b];
+  double AB2 = 0;
+  for (int x = 0; x < 3; ++x) AB2 += (A[x] - B[x]) * (A[x] - B[x]);
+  const double ABn = std::sqrt(AB2);
+  for (int ia = 0; ia < ctx->hnprim[a]; ++ia)
+    for (int ib = 0; ib < ctx->hnprim[b]; ++ib) {
+      double al = ctx->halpha[ctx->hpoff[a] + ia], be = ctx->halpha[ctx->hpoff[b] + ib];
+      double ca = ctx->hcoef[ctx->hpoff[a] + ia], cb = ctx->hcoef[ctx->hpoff[b] + ib];
+      double p = al + be;
+      double K = ca * cb * std::exp(-al * be / p * AB2);
+      if (prim_thresh > 0) {
+        double bound = std::fabs(K) * s2pi52 / (p * std::pow(2.0 * p, 0.25)) * std::pow(1.0 + ABn, ctx->hL[a] + ctx->hL[b]);
+        if (bound < prim_thresh) continue;
+      }
+      PrimPair pp;
+      pp.p = p;
+      pp.ip = 1.0 / p;
+      pp.Kp = s2pi52 * K / p;
+      pp.Px = (al * A[0] + be * B[0]) / p;
+      pp.Py = (al * A[1] + be * B[1]) / p;
+      pp.Pz = (al * A[2] + be * B[2]) / p;
+      out.push_back(pp);
+    }
+}
+
+// primitive-count bucket of a shell pair: warps of the ERI kernels see kets of one bucket
+static inline int prim_bucket(int np) {
+  if (np <= 1) return 0;
+  if (np <= 2) return 1;
+  if (np <= 4) return 2;
+  if (np <= 8) return 3;
+  if (np <= 16) return 4;
+  if (np <= 32) return 5;
+  if (np <= 64) return 6;
+  return 7;
+}
+
+// build primitive-pair data for the current pair ordering and upload all pair arrays
 static cqg_status upload_pairs(cqg_ctx *ctx, double prim_thresh) {
   size_t np = ctx->pair_sh.size();
-  std::vector<int> poff(np), npr(np);
+  std::vector<int> poff(np), npr(np), kk(np);
   std::vector<PrimPair> prim;
   prim.reserve(np * 4);
-  const double pi = 3.14159265358979323846;
   for (size_t i = 0; i < np; ++i) {
     int a = ctx->pair_sh[i].x, b = ctx->pair_sh[i].y;
-    const double *A = &ctx->hcent[3 * a], *B = &ctx->hcent[3 * b];
-    double AB2 = 0, ABn;
-    for (int x = 0; x < 3; ++x) AB2 += (A[x] - B[x]) * (A[x] - B[x]);
-    ABn = std::sqrt(AB2);
     poff[i] = (int)prim.size();
-    for (int ia = 0; ia < ctx->hnprim[a]; ++ia)
-      for (int ib = 0; ib < ctx->hnprim[b]; ++ib) {
-        double al = ctx->halpha[ctx->hpoff[a] + ia], be = ctx->halpha[ctx->hpoff[b] + ib];
-        double ca = ctx->hcoef[ctx->hpoff[a] + ia], cb = ctx->hcoef[ctx->hpoff[b] + ib];
-        double p = al + be;
-        double K = ca * cb * std::exp(-al * be / p * AB2);
-        if (prim_thresh > 0) {
-          // s-type sqrt((ij|ij)) estimate with a polynomial allowance for higher L
-          double bound = std::fabs(K) * std::sqrt(2.0 * std::pow(pi, 2.5)) / (p * std::pow(2.0 * p, 0.25)) *
-                         std::pow(1.0 + ABn, ctx->hL[a] + ctx->hL[b]);
-          if (bound < prim_thresh) continue;
-        }
-        PrimPair pp;
-        pp.p = p;
-        pp.K = K;
-        pp.Px = (al * A[0] + be * B[0]) / p;
-        pp.Py = (al * A[1] + be * B[1]) / p;
-        pp.Pz = (al * A[2] + be * B[2]) / p;
-        pp.pad = 0;
-        prim.push_back(pp);
-      }
+    kk[i] = ctx->hnprim[a] * ctx->hnprim[b];
+    pair_prims(ctx, a, b, prim_thresh, prim);
     npr[i] = (int)prim.size() - poff[i];
   }
   ctx->prim_pairs_total = (long long)prim.size();
   ctx->pair_np_host = npr;
   if (ctx->d_pair_sh.reserve(np) || ctx->d_pair_Q.reserve(np) || ctx->d_pair_poff.reserve(np) ||
-      ctx->d_pair_np.reserve(np) || ctx->d_prim.reserve(prim.size())) {
+      ctx->d_pair_np.reserve(np) || ctx->d_pair_kk.reserve(np) || ctx->d_prim.reserve(prim.size())) {
     ctx->err = "device allocation for pair data failed";
     return CQG_ERR_OOM;
   }
@@ -571,6 +978,7 @@ static cqg_status upload_pairs(cqg_ctx *ctx, double prim_thresh) {
   CUCHK(cudaMemcpy(ctx->d_pair_Q.p, ctx->pair_Q.data(), np * sizeof(double), cudaMemcpyHostToDevice));
   CUCHK(cudaMemcpy(ctx->d_pair_poff.p, poff.data(), np * sizeof(int), cudaMemcpyHostToDevice));
   CUCHK(cudaMemcpy(ctx->d_pair_np.p, npr.data(), np * sizeof(int), cudaMemcpyHostToDevice));
+  CUCHK(cudaMemcpy(ctx->d_pair_kk.p, kk.data(), np * sizeof(int), cudaMemcpyHostToDevice));
   if (!prim.empty())
     CUCHK(cudaMemcpy(ctx->d_prim.p, prim.data(), prim.size() * sizeof(PrimPair), cudaMemcpyHostToDevice));
   return CQG_OK;
@@ -581,10 +989,14 @@ typedef cudaError_t (*eri_launcher)(cqg_ctx *, int blk, long long n, cudaStream_
 template <int LA, int LB, int LC, int LD>
 static cudaError_t launch_eri(cqg_ctx *ctx, int blk, long long n, cudaStream_t st, const DigestGroups &dg) {
   if (n <= 0) return cudaSuccess;
-  long long nb = (n + 127) / 128;
-  k_eri_jk<LA, LB, LC, LD><<<(unsigned)nb, 128, 0, st>>>(ctx->d_qlist.p, ctx->d_range.p, blk, make_pairs(ctx),
-                                                         make_shells(ctx), ctx->d_boys.p, dg);
-  return cudaGetLastError();
+  if constexpr (is_warp_class(LA, LB, LC, LD)) {
+    return launch_warp<LA, LB, LC, LD, false>(ctx, blk, n, 0, 0, st, dg, nullptr);
+  } else {
+    long long nb = std::min<long long>((n + 127) / 128, 148LL * 12);
+    k_eri_jk<LA, LB, LC, LD><<<(unsigned)nb, 128, 0, st>>>(ctx->d_qlist.p, ctx->d_range.p, blk, make_pairs(ctx),
+                                                           make_shells(ctx), ctx->d_boys.p, dg);
+    return cudaGetLastError();
+  }
 }
 
 #define QC(a, b, c, d) &launch_eri<a, b, c, d>
@@ -661,6 +1073,7 @@ cqg_status cqg_destroy(cqg_ctx *ctx) {
   cudaSetDevice(ctx->device);
   ctx->d_center.release(); ctx->d_bf.release(); ctx->d_sz.release();
   ctx->d_pair_sh.release(); ctx->d_pair_Q.release(); ctx->d_pair_poff.release(); ctx->d_pair_np.release();
+  ctx->d_pair_kk.release(); ctx->d_blkacc.release();
   ctx->d_prim.release(); ctx->d_boys.release();
   ctx->d_M.release(); ctx->d_Mmax.release(); ctx->d_flags.release();
   ctx->d_cnt.release(); ctx->d_off.release(); ctx->d_range.release(); ctx->d_scan_tmp.release();
@@ -787,12 +1200,30 @@ cqg_status cqg_set_basis(cqg_ctx *ctx, int nshell, const int *L, const int *pure
     ctx->Qmat[a + (size_t)b * nshell] = ctx->pair_Q[i];
     ctx->Qmat[b + (size_t)a * nshell] = ctx->pair_Q[i];
   }
-  // sort each class by Q descending (stable) and rebuild with primitive-pair screening
+  // sort each class by (primitive-count bucket, Q descending), stable, and rebuild with
+  // primitive-pair screening; bucket starts go to the block table
+  std::vector<int> npscr(ctx->pair_sh.size());
+  {
+    std::vector<PrimPair> tmp;
+    for (size_t i = 0; i < ctx->pair_sh.size(); ++i) {
+      tmp.clear();
+      pair_prims(ctx, ctx->pair_sh[i].x, ctx->pair_sh[i].y, 1e-24, tmp);
+      npscr[i] = (int)tmp.size();
+    }
+  }
   for (int c = 0; c < CQG_NPC; ++c) {
     int b0 = ctx->pc_beg[c], b1 = ctx->pc_beg[c + 1];
     std::vector<int> idx(b1 - b0);
     std::iota(idx.begin(), idx.end(), b0);
-    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return ctx->pair_Q[x] > ctx->pair_Q[y]; });
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
+      int bx = prim_bucket(npscr[x]), by = prim_bucket(npscr[y]);
+      if (bx != by) return bx < by;
+      return ctx->pair_Q[x] > ctx->pair_Q[y];
+    });
+    for (int bk = 0; bk <= CQG_NBUCKET; ++bk) ctx->bucket_beg[c][bk] = b1;
+    for (int k = (int)idx.size() - 1; k >= 0; --k) ctx->bucket_beg[c][prim_bucket(npscr[idx[k]])] = b0 + k;
+    for (int bk = CQG_NBUCKET - 1; bk >= 0; --bk)
+      if (ctx->bucket_beg[c][bk] > ctx->bucket_beg[c][bk + 1]) ctx->bucket_beg[c][bk] = ctx->bucket_beg[c][bk + 1];
     std::vector<int2> sh2;
     std::vector<double> q2;
     for (int i : idx) {
@@ -815,6 +1246,7 @@ cqg_status cqg_set_basis(cqg_ctx *ctx, int nshell, const int *L, const int *pure
     bt.bra_beg[k] = ctx->pc_beg[i];
     bt.ket_beg[k] = ctx->pc_beg[j];
     bt.ket_n[k] = ctx->pc_beg[j + 1] - ctx->pc_beg[j];
+    for (int bk = 0; bk <= CQG_NBUCKET; ++bk) bt.ket_bucket[k][bk] = ctx->bucket_beg[j][bk];
     bt.diag[k] = (i == j);
     task += ctx->pc_beg[i + 1] - ctx->pc_beg[i];
   }
@@ -825,7 +1257,7 @@ cqg_status cqg_set_basis(cqg_ctx *ctx, int nshell, const int *L, const int *pure
   cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (long long *)nullptr, (long long *)nullptr, std::max(task, 1));
   if (ctx->d_cnt.reserve(task + 1) || ctx->d_off.reserve(task + 1) || ctx->d_range.reserve(2 * CQG_NQC) ||
       ctx->d_scan_tmp.reserve(scan_bytes + 16) || ctx->d_M.reserve((size_t)nshell * nshell) ||
-      ctx->d_Mmax.reserve(1) || ctx->d_flags.reserve(4))
+      ctx->d_Mmax.reserve(1) || ctx->d_flags.reserve(4) || ctx->d_blkacc.reserve(2 * CQG_NQC))
     return CQG_ERR_OOM;
   return CQG_OK;
 }
@@ -848,6 +1280,8 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
   for (int i = 0; i < nx_all; ++i) xl.X[i] = Xall[i];
   CUCHK(cudaMemsetAsync(ctx->d_flags.p, 0, 4 * sizeof(int), st));
   CUCHK(cudaMemsetAsync(ctx->d_Mmax.p, 0, sizeof(double), st));
+  CUCHK(cudaMemsetAsync(ctx->d_blkacc.p, 0, 2 * CQG_NQC * sizeof(unsigned long long), st));
+  ctx->launches = 0;
   {
     dim3 g((nsh + 127) / 128, nsh);
     k_blocknorm<<<g, 128, 0, st>>>(xl, ldx, nsh, ctx->d_bf.p, ctx->d_sz.p, ctx->d_M.p, ctx->d_flags.p, 1e-12);
@@ -856,6 +1290,7 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     int nb = (int)std::min<long long>((nn + 255) / 256, 1184);
     k_maxreduce<<<nb, 256, 0, st>>>(ctx->d_M.p, nn, ctx->d_Mmax.p);
     CUCHK(cudaGetLastError());
+    ctx->launches += 2;
   }
   // 2. quartet lists
   Pairs P = make_pairs(ctx);
@@ -863,16 +1298,19 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     int nthr = 256, wpb = nthr / 32;
     int nb = (ctx->ntask + wpb - 1) / wpb;
     k_quartets<false><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, nsh, ctx->d_Mmax.p, ctx->thresh,
-                                            ctx->d_cnt.p, nullptr, nullptr);
+                                            ctx->d_cnt.p, nullptr, nullptr, ctx->d_blkacc.p);
     CUCHK(cudaGetLastError());
     size_t scan_bytes = ctx->d_scan_tmp.n;
     CUCHK(cub::DeviceScan::ExclusiveSum(ctx->d_scan_tmp.p, scan_bytes, ctx->d_cnt.p, ctx->d_off.p, ctx->ntask, st));
     k_block_ranges<<<1, 64, 0, st>>>(ctx->bt, ctx->d_cnt.p, ctx->d_off.p, ctx->d_range.p);
     CUCHK(cudaGetLastError());
+    ctx->launches += 2;
   }
   long long hr[2 * CQG_NQC];
+  unsigned long long hacc[2 * CQG_NQC];
   int hflags[4];
   CUCHK(cudaMemcpyAsync(hr, ctx->d_range.p, sizeof(hr), cudaMemcpyDeviceToHost, st));
+  CUCHK(cudaMemcpyAsync(hacc, ctx->d_blkacc.p, sizeof(hacc), cudaMemcpyDeviceToHost, st));
   CUCHK(cudaMemcpyAsync(hflags, ctx->d_flags.p, sizeof(hflags), cudaMemcpyDeviceToHost, st));
   CUCHK(cudaStreamSynchronize(st));
   if (hflags[0]) {
@@ -892,8 +1330,9 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     int nthr = 256, wpb = nthr / 32;
     int nb = (ctx->ntask + wpb - 1) / wpb;
     k_quartets<true><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, nsh, ctx->d_Mmax.p, ctx->thresh,
-                                           nullptr, ctx->d_off.p, ctx->d_qlist.p);
+                                           nullptr, ctx->d_off.p, ctx->d_qlist.p, nullptr);
     CUCHK(cudaGetLastError());
+    ctx->launches += 1;
   }
   if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[1], st));
   // 3. ERI + digest per class
@@ -919,8 +1358,10 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     ctx->stats.class_quartets[k] = nq;
     int i, j;
     qclass_split(k, i, j);
-    (void)i;
-    (void)j;
+    const int la = kPairClass[i][0], lb = kPairClass[i][1], lc = kPairClass[j][0], ld = kPairClass[j][1];
+    mflops += (double)hacc[2 * k] * md_v1_prim_flops(la, lb, lc, ld) + (double)nq * md_v1_digest_flops(la, lb, lc, ld);
+    nprimq += (long long)hacc[2 * k + 1];
+    if (nq > 0) ctx->launches += 1;
     if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[4 + 2 * k], st));
     cudaError_t e = kEriLaunch[k](ctx, k, nq, st, dg);
     if (e != cudaSuccess) {
@@ -935,12 +1376,14 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     dim3 grid((n + 31) / 32, (n + 31) / 32), blk(32, 8);
     k_finalize<<<grid, blk, 0, st>>>(dg.G[g], n, AXg[g], ldax);
     CUCHK(cudaGetLastError());
+    ctx->launches += 1;
   }
   if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[3], st));
   ctx->stats.quartets = total;
   ctx->stats.quartets_fp32 = 0;
-  (void)mflops;
-  (void)nprimq;
+  ctx->stats.model_flops = mflops;
+  ctx->stats.prim_quartets = nprimq;
+  ctx->stats.launches = ctx->launches;
   return CQG_OK;
 }
 
@@ -1065,15 +1508,6 @@ cqg_status cqg_get_stats(cqg_ctx *ctx, cqg_stats *out) {
   CUCHK(cudaSetDevice(ctx->device));
   CUCHK(cudaDeviceSynchronize());
   cqg_stats &s = ctx->stats;
-  double mf = 0;
-  for (int k = 0; k < CQG_NQC; ++k) {
-    int i, j;
-    qclass_split(k, i, j);
-    int la = kPairClass[i][0], lb = kPairClass[i][1], lc = kPairClass[j][0], ld = kPairClass[j][1];
-    (void)la;
-    mf += (double)s.class_quartets[k] * md_v1_digest_flops(la, lb, lc, ld);
-  }
-  (void)mf;
   if (ctx->timing) {
     float ms;
     cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);

@@ -4,10 +4,12 @@
 #include <stdint.h>
 
 // One primitive pair of a shell pair (Gaussian product theorem data).
-//   p = alpha_a + alpha_b, P = (alpha_a A + alpha_b B) / p,
-//   K = c_a c_b exp(-alpha_a alpha_b / p |A-B|^2)   (normalised contraction coefficients)
+//   p = alpha_a + alpha_b, ip = 1/p, P = (alpha_a A + alpha_b B) / p,
+//   Kp = sqrt(2 pi^(5/2)) c_a c_b exp(-alpha_a alpha_b / p |A-B|^2) / p
+// so that the primitive-quartet prefactor 2 pi^(5/2) K_ab K_cd / (p q sqrt(p+q)) is
+// Kp_ab * Kp_cd * rsqrt(p+q)  (c_a, c_b: normalised contraction coefficients).
 struct __align__(16) PrimPair {
-  double p, K, Px, Py, Pz, pad;
+  double p, Kp, Px, Py, Pz, ip;
 };
 
 #define TWO_PI_2P5 34.986836655249725   // 2 pi^(5/2)
@@ -33,6 +35,43 @@ __device__ __forceinline__ void boys_eval(double T, const double* __restrict__ t
     double f = __ldg(row + BOYS_NTAYLOR);
 #pragma unroll
     for (int k = BOYS_NTAYLOR; k >= 1; --k) f = __ldg(row + k - 1) + x * f * (1.0 / k);
+    F[L] = f;
+    if (L > 0) {
+      const double e = exp(-T);
+      const double t2 = 2.0 * T;
+#pragma unroll
+      for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * (1.0 / (2 * m + 1));
+    }
+  } else {
+    F[0] = 0.5 * sqrt(3.141592653589793 / T);
+    if (L > 0) {
+      const double e = exp(-T);
+      const double i2t = 0.5 / T;
+#pragma unroll
+      for (int m = 0; m < L; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) * i2t;
+    }
+  }
+}
+
+// Shared-memory copy of the rows a kernel of total angular momentum L needs:
+// s[i * BOYS_SROW + k] = F_{L+k}(0.1 i), k = 0..BOYS_NTAYLOR.
+#define BOYS_SROW (BOYS_NTAYLOR + 1)
+template <int L>
+__device__ __forceinline__ void stage_boys(const double *__restrict__ tab, double *s) {
+  for (int k = threadIdx.x; k < BOYS_NT * BOYS_SROW; k += blockDim.x)
+    s[k] = __ldg(tab + (k / BOYS_SROW) * BOYS_NORD + L + (k % BOYS_SROW));
+}
+
+// boys_eval with the table staged in shared memory (layout of stage_boys<L>)
+template <int L>
+__device__ __forceinline__ void boys_eval_sm(double T, const double *s, double *F) {
+  if (T < BOYS_TMAX) {
+    const int i = __double2int_rn(T * 10.0);
+    const double x = (double)i * 0.1 - T;
+    const double *row = s + i * BOYS_SROW;
+    double f = row[BOYS_NTAYLOR];
+#pragma unroll
+    for (int k = BOYS_NTAYLOR; k >= 1; --k) f = row[k - 1] + x * f * (1.0 / k);
     F[L] = f;
     if (L > 0) {
       const double e = exp(-T);

@@ -10,7 +10,8 @@ class not below the ket pair class, this emits one fully unrolled device functio
                                          const double* boys_tab, T* out)
 
 that returns the contracted, normalised (ab|cd) over the reference's basis functions
-(spherical for pure shells) in row-major [a][b][c][d] order.
+(spherical for pure shells) in row-major [a][b][c][d] order.  ``boys_tab`` is the
+shared-memory Boys table of ``stage_boys<L>`` (eri_common.cuh), L = la+lb+lc+ld.
 
 Method (McMurchie & Davidson, J. Comput. Phys. 26, 218 (1978); notation of Helgaker,
 Jorgensen & Olsen ch. 9.5 and 9.9):
@@ -195,7 +196,7 @@ def gen_class(la, lb, lc, ld, pa, pb, pc, pd):
     g.ind += 1
     g.w("const PrimPair pb = bra[ib];")
     g.w("const double p = pb.p;")
-    g.w("const T bo2p = T(0.5 / p);")
+    g.w("const T bo2p = T(0.5 * pb.ip);")
     for d, comp in zip("xyz", "xyz"):
         g.w("const T bPA%s = T(pb.P%s - A.%s);" % (d, comp, comp))
         g.w("const T bPB%s = T(pb.P%s - B.%s);" % (d, comp, comp))
@@ -208,11 +209,14 @@ def gen_class(la, lb, lc, ld, pa, pb, pc, pd):
     for h in range(len(hp)):
         for c in range(ncd):
             g.w("T W%d_%d = T(0);" % (h, c))
+    g.w("PrimPair pk_next;")
+    g.w("if (nket > 0) pk_next = ket[0];")
     g.w("for (int ik = 0; ik < nket; ++ik) {")
     g.ind += 1
-    g.w("const PrimPair pk = ket[ik];")
+    g.w("const PrimPair pk = pk_next;")
+    g.w("if (ik + 1 < nket) pk_next = ket[ik + 1];")
     g.w("const double q = pk.p;")
-    g.w("const T ko2p = T(0.5 / q);")
+    g.w("const T ko2p = T(0.5 * pk.ip);")
     for d in "xyz":
         g.w("const T kPA%s = T(pk.P%s - C.%s);" % (d, d, d))
         g.w("const T kPB%s = T(pk.P%s - D.%s);" % (d, d, d))
@@ -223,12 +227,13 @@ def gen_class(la, lb, lc, ld, pa, pb, pc, pd):
                 needk[d].add((c[k], dd[k]))
     emit_E(g, "k", lc, ld, needk)
     g.w("const double pq = p + q;")
-    g.w("const double rho = p * q / pq;")
+    g.w("const double rpq = rsqrt(pq);")
+    g.w("const double rho = p * q * (rpq * rpq);")
     g.w("const double PQx = pb.Px - pk.Px, PQy = pb.Py - pk.Py, PQz = pb.Pz - pk.Pz;")
     g.w("const double Tb = rho * (PQx * PQx + PQy * PQy + PQz * PQz);")
     g.w("double F[%d];" % (L + 1))
-    g.w("boys_eval<%d>(Tb, boys_tab, F);" % L)
-    g.w("const double pref = TWO_PI_2P5 / (p * q * sqrt(pq)) * pb.K * pk.K;")
+    g.w("boys_eval_sm<%d>(Tb, boys_tab, F);" % L)
+    g.w("const double pref = pb.Kp * pk.Kp * rpq;")
     # R^n_000
     g.w("const double m2r = -2.0 * rho;")
     g.w("double fac = pref;")
@@ -342,12 +347,27 @@ def quartet_classes(maxl):
     return out
 
 
+# classes evaluated by the warp-cooperative kernel (eri_warp.cuh): their Cartesian output
+# ncart(a)ncart(b)ncart(c)ncart(d) exceeds 150 values, too many for one thread's registers
+def _nc(l):
+    return (l + 1) * (l + 2) // 2
+
+
+WARP_CLASSES = {q for q in quartet_classes(3) if _nc(q[0]) * _nc(q[1]) * _nc(q[2]) * _nc(q[3]) > 150}
+
+
 def main(path, maxl=2):
     parts = ["// GENERATED by gen_eri.py -- do not edit.",
              "#pragma once",
              "#include \"../eri_common.cuh\"",
              ""]
+    for l in (2, 3):
+        M = solid_harmonic_matrix(l)
+        parts.append("__constant__ double kSph%d[%d] = {%s};" % (l, M.size, ", ".join(repr(float(x)) for x in M.ravel())))
+    parts.append("")
     for (la, lb, lc, ld) in quartet_classes(maxl):
+        if (la, lb, lc, ld) in WARP_CLASSES:
+            continue
         _, code = gen_class(la, lb, lc, ld, la > 1, lb > 1, lc > 1, ld > 1)
         parts.append(code)
         parts.append("template <> struct EriClass<%d, %d, %d, %d> {" % (la, lb, lc, ld))

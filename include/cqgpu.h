@@ -57,6 +57,7 @@ typedef struct {
   double ms_screen;                /* device time of screening + list build (ms) */
   double ms_eri;                   /* device time of ERI + digest kernels (ms) */
   double ms_total;                 /* device time of the whole call (ms) */
+  long long launches;              /* kernels of this library launched by the call */
   long long class_quartets[55];    /* per quartet class (index: see cqg_class_name) */
   double class_ms[55];             /* device time per class kernel (ms), if timing on */
 } cqg_stats;

@@ -424,13 +424,14 @@ void oracle_shblk_norm(int nshell, const int *L, const int *pure, const double *
  * `nthreads` <= 0 uses the OpenMP default; the round-robin split is s1234 % nthreads
  * exactly as contract.h:107 does.  If `per_class` is non-NULL it receives the screened
  * quartet count per (la,lb,lc,ld) in shell-index orientation, indexed
- * ((la*5+lb)*5+lc)*5+ld. */
+ * ((la*5+lb)*5+lc)*5+ld.  s1_begin/s1_end (-1 = all) restrict the outermost shell index,
+ * which the benchmark uses to time a bounded slice of a large workload. */
 long long oracle_twoe_contract_direct(int nshell, const int *L, const int *pure, const int *nprim,
                                       const double *alpha, const double *coef, const double *centers,
                                       const double *const *sph, const double *Q, double thresh,
                                       int nmat, const double *const *X, double *const *AX,
                                       const int *types, const double *scale, int ld, int nthreads,
-                                      long long *per_class) {
+                                      long long *per_class, int s1_begin, int s1_end) {
   obasis B; obasis_init(&B, nshell, L, pure, nprim, alpha, coef, centers, sph);
   size_t nbf = B.nbf;
   double **blk = (double **)malloc(sizeof(double *) * nmat);
@@ -457,8 +458,15 @@ long long oracle_twoe_contract_direct(int nshell, const int *L, const int *pure,
     eri_ws *w = eri_ws_new();
     double *buff = (double *)malloc(sizeof(double) * 7 * 7 * 7 * 7 * 16);
     unsigned long s1234 = 0;
+    if (s1_end < 0 || s1_end > nshell) s1_end = nshell;
+    if (s1_begin < 0) s1_begin = 0;
     for (int s1 = 0; s1 < nshell; s1++) {
       size_t bf1_s = B.bfoff[s1]; int n1 = B.size[s1];
+      if (s1 < s1_begin || s1 >= s1_end) {  /* bounded sample: keep the global counter */
+        unsigned long m = (unsigned long)s1;
+        s1234 += (m + 1) * (m * (m + 1) / 2) + (m + 1) * (m + 2) / 2;
+        continue;
+      }
       for (int s2 = 0; s2 <= s1; s2++) {
         size_t bf2_s = B.bfoff[s2]; int n2 = B.size[s2];
         for (int s3 = 0; s3 <= s1; s3++) {
@@ -603,9 +611,9 @@ void oracle_one_e(int nshell, const int *L, const int *pure, const int *nprim,
           for (int x = 0; x < 3; x++) os_overlap_1d(P[x] - A[x], P[x] - Bc[x], p, la + 1, lb + 2, S1[x], 8);
           /* overlap + kinetic */
           for (int ia = 0; ia < nca; ia++) {
-            int ax[3]; { int ii = 0, c = 0; for (int i1 = 0; i1 <= la; i1++) for (int j1 = 0; j1 <= i1; j1++, c++) if (c == ia) { ax[0] = la - i1; ax[1] = i1 - j1; ax[2] = j1; ii = 1; } (void)ii; }
+            int ax[3] = {0, 0, 0}; { int ii = 0, c = 0; for (int i1 = 0; i1 <= la; i1++) for (int j1 = 0; j1 <= i1; j1++, c++) if (c == ia) { ax[0] = la - i1; ax[1] = i1 - j1; ax[2] = j1; ii = 1; } (void)ii; }
             for (int ib = 0; ib < ncb; ib++) {
-              int bx[3]; { int c = 0; for (int i1 = 0; i1 <= lb; i1++) for (int j1 = 0; j1 <= i1; j1++, c++) if (c == ib) { bx[0] = lb - i1; bx[1] = i1 - j1; bx[2] = j1; } }
+              int bx[3] = {0, 0, 0}; { int c = 0; for (int i1 = 0; i1 <= lb; i1++) for (int j1 = 0; j1 <= i1; j1++, c++) if (c == ib) { bx[0] = lb - i1; bx[1] = i1 - j1; bx[2] = j1; } }
               double s[3], t[3];
               for (int x = 0; x < 3; x++) {
                 int ii = ax[x], jj = bx[x];
