@@ -29,7 +29,7 @@ EXPORTED = [
     "cqg_version", "cqg_status_string", "cqg_create", "cqg_destroy", "cqg_last_error",
     "cqg_set_basis", "cqg_set_threshold", "cqg_set_precision", "cqg_get_schwarz",
     "cqg_get_sizes", "cqg_twoe_contract_direct", "cqg_form_pt", "cqg_get_stats",
-    "cqg_set_timing", "cqg_class_name", "cqg_probe_fma_peak",
+    "cqg_set_timing", "cqg_class_name", "cqg_probe_fma_peak", "cqg_one_e",
 ]
 
 
@@ -77,9 +77,10 @@ def load(path: str = LIB_PATH):
     L.cqg_class_name.argtypes = [ctypes.c_int]
     L.cqg_class_name.restype = ctypes.c_char_p
     L.cqg_probe_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, d]
+    L.cqg_one_e.argtypes = [vp, ctypes.c_int, d, d, vp, vp, vp, ctypes.c_int, ctypes.c_int, vp]
     for name in ["cqg_create", "cqg_destroy", "cqg_set_basis", "cqg_set_threshold", "cqg_set_precision",
                  "cqg_get_schwarz", "cqg_get_sizes", "cqg_twoe_contract_direct", "cqg_form_pt",
-                 "cqg_get_stats", "cqg_set_timing", "cqg_probe_fma_peak"]:
+                 "cqg_get_stats", "cqg_set_timing", "cqg_probe_fma_peak", "cqg_one_e"]:
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

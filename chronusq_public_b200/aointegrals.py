@@ -195,6 +195,28 @@ class AOIntegrals:
         _lib.check(st, self._ctx)
         return PTs, (None if is_rhf else PTz)
 
+    def computeAOOneE(self, charges, coords_bohr, device_out: bool = False):
+        """Overlap, kinetic and nuclear-attraction matrices (AOIntegrals::computeAOOneE,
+        src/aointegrals/aointegrals_builders.cpp:337-467), evaluated on the GPU.
+        Returns (S, T, V) as CUDA torch tensors when ``device_out`` else numpy arrays."""
+        n = self.nBasis
+        Z = np.ascontiguousarray(charges, dtype=np.float64)
+        R = np.ascontiguousarray(coords_bohr, dtype=np.float64).reshape(-1, 3)
+        d = ctypes.POINTER(ctypes.c_double)
+        if device_out:
+            import torch
+            S, T, V = (torch.zeros((n, n), dtype=torch.float64, device="cuda:%d" % self.device) for _ in range(3))
+            ptrs = [ctypes.c_void_p(x.data_ptr()) for x in (S, T, V)]
+            mode = 1
+        else:
+            S, T, V = (np.zeros((n, n), order="F") for _ in range(3))
+            ptrs = [ctypes.c_void_p(x.ctypes.data) for x in (S, T, V)]
+            mode = 0
+        st = self._L.cqg_one_e(self._ctx, len(Z), Z.ctypes.data_as(d), R.ctypes.data_as(d), ptrs[0], ptrs[1],
+                               ptrs[2], n, mode, self._stream(mode))
+        _lib.check(st, self._ctx)
+        return S, T, V
+
     @staticmethod
     def _like(x):
         if _is_torch(x):

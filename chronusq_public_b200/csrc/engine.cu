@@ -27,6 +27,7 @@
 #include "eri_common.cuh"
 #include "_gen/eri_classes.cuh"
 #include "eri_warp.cuh"
+#include "one_e.cuh"
 
 #define CQG_MAXL 2
 #define CQG_NPC ((CQG_MAXL + 1) * (CQG_MAXL + 2) / 2)       // pair classes
@@ -816,6 +817,11 @@ struct cqg_ctx {
   DevBuf<int2> d_pair_sh;
   DevBuf<double> d_pair_Q;
   DevBuf<int> d_pair_poff, d_pair_np, d_pair_kk;
+  DevBuf<int> d_shL, d_shnp, d_shpoff;
+  DevBuf<double> d_alpha, d_coef;
+  DevBuf<int2> d_allpairs;
+  DevBuf<double> d_oe;       // host-mode staging of S, T, V
+  DevBuf<double> d_charges;  // Z then R (3 per charge)
   DevBuf<unsigned long long> d_blkacc;
   int launches = 0;
   DevBuf<PrimPair> d_prim;
@@ -1074,6 +1080,8 @@ cqg_status cqg_destroy(cqg_ctx *ctx) {
   ctx->d_center.release(); ctx->d_bf.release(); ctx->d_sz.release();
   ctx->d_pair_sh.release(); ctx->d_pair_Q.release(); ctx->d_pair_poff.release(); ctx->d_pair_np.release();
   ctx->d_pair_kk.release(); ctx->d_blkacc.release();
+  ctx->d_shL.release(); ctx->d_shnp.release(); ctx->d_shpoff.release(); ctx->d_alpha.release();
+  ctx->d_coef.release(); ctx->d_allpairs.release(); ctx->d_oe.release(); ctx->d_charges.release();
   ctx->d_prim.release(); ctx->d_boys.release();
   ctx->d_M.release(); ctx->d_Mmax.release(); ctx->d_flags.release();
   ctx->d_cnt.release(); ctx->d_off.release(); ctx->d_range.release(); ctx->d_scan_tmp.release();
@@ -1160,6 +1168,21 @@ cqg_status cqg_set_basis(cqg_ctx *ctx, int nshell, const int *L, const int *pure
   CUCHK(cudaMemcpy(ctx->d_center.p, c3.data(), nshell * sizeof(double3), cudaMemcpyHostToDevice));
   CUCHK(cudaMemcpy(ctx->d_bf.p, ctx->hbf.data(), nshell * sizeof(int), cudaMemcpyHostToDevice));
   CUCHK(cudaMemcpy(ctx->d_sz.p, ctx->hsz.data(), nshell * sizeof(int), cudaMemcpyHostToDevice));
+  // raw shells (one-electron integrals) and the list of all pairs a >= b
+  {
+    std::vector<int2> allp;
+    for (int a = 0; a < nshell; ++a)
+      for (int b = 0; b <= a; ++b) allp.push_back(make_int2(a, b));
+    if (ctx->d_shL.reserve(nshell) || ctx->d_shnp.reserve(nshell) || ctx->d_shpoff.reserve(nshell) ||
+        ctx->d_alpha.reserve(tot) || ctx->d_coef.reserve(tot) || ctx->d_allpairs.reserve(allp.size()))
+      return CQG_ERR_OOM;
+    CUCHK(cudaMemcpy(ctx->d_shL.p, L, nshell * sizeof(int), cudaMemcpyHostToDevice));
+    CUCHK(cudaMemcpy(ctx->d_shnp.p, nprim, nshell * sizeof(int), cudaMemcpyHostToDevice));
+    CUCHK(cudaMemcpy(ctx->d_shpoff.p, ctx->hpoff.data(), nshell * sizeof(int), cudaMemcpyHostToDevice));
+    CUCHK(cudaMemcpy(ctx->d_alpha.p, alpha, tot * sizeof(double), cudaMemcpyHostToDevice));
+    CUCHK(cudaMemcpy(ctx->d_coef.p, coef, tot * sizeof(double), cudaMemcpyHostToDevice));
+    CUCHK(cudaMemcpy(ctx->d_allpairs.p, allp.data(), allp.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  }
   // pairs by class, internal orientation L_a >= L_b (a >= b when equal L)
   std::vector<std::vector<int2>> bycls(CQG_NPC);
   for (int a = 0; a < nshell; ++a)
@@ -1501,6 +1524,59 @@ cqg_status cqg_form_pt(cqg_ctx *ctx, int is_rhf, double xHF, const double *Ps, c
   int types[3] = {CQG_COULOMB, CQG_EXCHANGE, CQG_EXCHANGE};
   double scale[3] = {1.0, xHF, xHF};
   return cqg_twoe_contract_direct(ctx, 3, X, AX, types, scale, ld, on_device, stream);
+}
+
+cqg_status cqg_one_e(cqg_ctx *ctx, int ncharge, const double *Z, const double *R, double *S, double *T, double *V,
+                     int ld, int on_device, void *stream) {
+  if (!ctx || ncharge < 0 || (ncharge > 0 && (!Z || !R)) || !S || !T || !V) return CQG_ERR_BAD_ARG;
+  if (ctx->nshell == 0) {
+    ctx->err = "cqg_set_basis has not been called";
+    return CQG_ERR_STATE;
+  }
+  const int n = ctx->nbf;
+  if (ld < n) return CQG_ERR_BAD_ARG;
+  CUCHK(cudaSetDevice(ctx->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  if (ctx->d_charges.reserve(4 * (size_t)std::max(ncharge, 1))) return CQG_ERR_OOM;
+  std::vector<double> zr(4 * (size_t)std::max(ncharge, 1), 0.0);
+  for (int c = 0; c < ncharge; ++c) {
+    zr[c] = Z[c];
+    zr[ncharge + 3 * c] = R[3 * c];
+    zr[ncharge + 3 * c + 1] = R[3 * c + 1];
+    zr[ncharge + 3 * c + 2] = R[3 * c + 2];
+  }
+  CUCHK(cudaMemcpyAsync(ctx->d_charges.p, zr.data(), zr.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  double *dS = S, *dT = T, *dV = V;
+  int ldd = ld;
+  if (!on_device) {
+    if (ctx->d_oe.reserve(3 * (size_t)n * n)) return CQG_ERR_OOM;
+    dS = ctx->d_oe.p;
+    dT = dS + (size_t)n * n;
+    dV = dT + (size_t)n * n;
+    ldd = n;
+  }
+  OneEShells sh;
+  sh.L = ctx->d_shL.p;
+  sh.nprim = ctx->d_shnp.p;
+  sh.poff = ctx->d_shpoff.p;
+  sh.bf = ctx->d_bf.p;
+  sh.alpha = ctx->d_alpha.p;
+  sh.coef = ctx->d_coef.p;
+  sh.center = ctx->d_center.p;
+  const int np = ctx->nshell * (ctx->nshell + 1) / 2;
+  k_one_e<<<(np + 63) / 64, 64, 0, st>>>(sh, ctx->d_allpairs.p, np, ncharge, ctx->d_charges.p,
+                                         (const double3 *)(ctx->d_charges.p + ncharge), ctx->d_boys.p, dS, dT, dV,
+                                         ldd);
+  CUCHK(cudaGetLastError());
+  if (!on_device) {
+    double *outs[3] = {S, T, V};
+    const double *ins[3] = {dS, dT, dV};
+    for (int q = 0; q < 3; ++q)
+      CUCHK(cudaMemcpy2DAsync(outs[q], ld * sizeof(double), ins[q], n * sizeof(double), n * sizeof(double), n,
+                              cudaMemcpyDeviceToHost, st));
+    CUCHK(cudaStreamSynchronize(st));
+  }
+  return CQG_OK;
 }
 
 cqg_status cqg_get_stats(cqg_ctx *ctx, cqg_stats *out) {

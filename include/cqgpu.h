@@ -111,6 +111,13 @@ cqg_status cqg_form_pt(cqg_ctx *ctx, int is_rhf, double xHF, const double *Ps,
                        const double *Pz, double *PTs, double *PTz, int ld, int on_device,
                        void *stream);
 
+/* One-electron integrals on the device: overlap S, kinetic T and nuclear attraction V
+ * of `ncharge` point charges Z at R (ncharge x 3, bohr), each nbf x nbf (leading dim
+ * `ld`), in the same basis-function order.  Replaces AOIntegrals::computeAOOneE's
+ * OneEDriver calls (src/aointegrals/aointegrals_builders.cpp:27-133, 337-467). */
+cqg_status cqg_one_e(cqg_ctx *ctx, int ncharge, const double *Z, const double *R, double *S,
+                     double *T, double *V, int ld, int on_device, void *stream);
+
 /* Statistics of the last contraction (synchronises the context's stream). */
 cqg_status cqg_get_stats(cqg_ctx *ctx, cqg_stats *out);
 /* Per-class kernel timing on (1) / off (0, default). */
