@@ -39,6 +39,7 @@ class CqgStats(ctypes.Structure):
         ("quartets_fp32", ctypes.c_longlong),
         ("prim_quartets", ctypes.c_longlong),
         ("model_flops", ctypes.c_double),
+        ("model_flops_fp32", ctypes.c_double),
         ("ms_screen", ctypes.c_double),
         ("ms_eri", ctypes.c_double),
         ("ms_total", ctypes.c_double),

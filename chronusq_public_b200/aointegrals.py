@@ -129,6 +129,7 @@ class AOIntegrals:
         return {
             "quartets": int(s.quartets), "quartets_fp32": int(s.quartets_fp32),
             "prim_quartets": int(s.prim_quartets), "model_flops": float(s.model_flops),
+            "model_flops_fp32": float(s.model_flops_fp32),
             "ms_screen": s.ms_screen, "ms_eri": s.ms_eri, "ms_total": s.ms_total,
             "launches": int(s.launches),
             "class_quartets": {names[k]: int(s.class_quartets[k]) for k in range(len(names))},

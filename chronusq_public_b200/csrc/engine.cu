@@ -192,8 +192,10 @@ __device__ __forceinline__ int coarse_range(const double *__restrict__ Q, int kb
   return lo;
 }
 
-__device__ __forceinline__ bool exact_pass(const double *__restrict__ M, int nsh, int2 ab, int2 cd,
-                                           double qab, double qcd, double thresh) {
+// Density-weighted Schwarz bound of a quartet: max of the six shell-block norms of the
+// density times Q_ab Q_cd (contract.h:112-131).
+__device__ __forceinline__ double quartet_bound(const double *__restrict__ M, int nsh, int2 ab, int2 cd, double qab,
+                                                double qcd) {
   const int s1 = ab.x, s2 = ab.y, s3 = cd.x, s4 = cd.y;
   double m = M[s1 + (size_t)s4 * nsh];
   m = fmax(m, M[s2 + (size_t)s4 * nsh]);
@@ -201,17 +203,19 @@ __device__ __forceinline__ bool exact_pass(const double *__restrict__ M, int nsh
   m = fmax(m, M[s1 + (size_t)s3 * nsh]);
   m = fmax(m, M[s2 + (size_t)s3 * nsh]);
   m = fmax(m, M[s1 + (size_t)s2 * nsh]);
-  return m * qab * qcd >= thresh;
+  return m * qab * qcd;
 }
 
 // Count (FILL=false) or write (FILL=true) the passing quartets of each task.  One warp
 // per task; ket pairs scanned in ascending order, survivors compacted with a ballot so
-// the list is deterministic.
+// the list is deterministic.  Quartets whose bound is below `cut32` go to the FP32 list
+// (counts cnt[ntask + task], offsets off[ntask + task]); the rest to the FP64 list.
 template <bool FILL>
 __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pairs P, const double *__restrict__ M,
                                                   int nsh, const double *__restrict__ Mmax, double thresh,
-                                                  long long *__restrict__ cnt, const long long *__restrict__ off,
-                                                  uint2 *__restrict__ qlist, unsigned long long *__restrict__ blkacc) {
+                                                  double cut32, long long *__restrict__ cnt,
+                                                  const long long *__restrict__ off, uint2 *__restrict__ qlist,
+                                                  unsigned long long *__restrict__ blkacc) {
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (warp >= ntask) return;
@@ -221,9 +225,9 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
   double mm = *Mmax;
   double cut = (qb * mm > 0.0) ? thresh / (qb * mm) * (1.0 - 1e-12) : 0.0;
   int2 ab = P.sh[bra];
-  long long base = FILL ? off[warp] : 0;
-  long long c = 0;
-  unsigned long long kmodel = 0, kexec = 0;
+  const long long base64 = FILL ? off[warp] : 0, base32 = FILL ? off[ntask + warp] : 0;
+  long long c64 = 0, c32 = 0;
+  unsigned long long km64 = 0, ke64 = 0, km32 = 0, ke32 = 0;
   if (qb * mm > 0.0) {
     for (int bk = 0; bk < CQG_NBUCKET; ++bk) {
       const int kb = bt.ket_bucket[blk][bk], ke = bt.ket_bucket[blk][bk + 1];
@@ -232,42 +236,60 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
       if (bt.diag[blk]) kend = min(kend, bra + 1);   // unique pairs of pairs: ket <= bra
       for (int k0 = kb; k0 < kend; k0 += 32) {
         int ket = k0 + lane;
-        bool pass = false;
-        if (ket < kend) pass = exact_pass(M, nsh, ab, P.sh[ket], qb, P.Q[ket], thresh);
-        unsigned bal = __ballot_sync(0xffffffffu, pass);
-        if (FILL && pass) {
-          int pos = __popc(bal & ((1u << lane) - 1u));
-          qlist[base + c + pos] = make_uint2((unsigned)bra, (unsigned)ket);
+        bool pass = false, lo = false;
+        if (ket < kend) {
+          const double bnd = quartet_bound(M, nsh, ab, P.sh[ket], qb, P.Q[ket]);
+          pass = bnd >= thresh;
+          lo = pass && bnd < cut32;
         }
-        if (!FILL && pass) {
-          kmodel += (unsigned long long)P.kk[ket];
-          kexec += (unsigned long long)P.np[ket];
+        const bool hi = pass && !lo;
+        unsigned b64 = __ballot_sync(0xffffffffu, hi), b32 = __ballot_sync(0xffffffffu, lo);
+        const unsigned below = (1u << lane) - 1u;
+        if (FILL && hi) qlist[base64 + c64 + __popc(b64 & below)] = make_uint2((unsigned)bra, (unsigned)ket);
+        if (FILL && lo) qlist[base32 + c32 + __popc(b32 & below)] = make_uint2((unsigned)bra, (unsigned)ket);
+        if (!FILL && hi) {
+          km64 += (unsigned long long)P.kk[ket];
+          ke64 += (unsigned long long)P.np[ket];
         }
-        c += __popc(bal);
+        if (!FILL && lo) {
+          km32 += (unsigned long long)P.kk[ket];
+          ke32 += (unsigned long long)P.np[ket];
+        }
+        c64 += __popc(b64);
+        c32 += __popc(b32);
       }
     }
   }
   if (!FILL) {
     for (int o = 16; o > 0; o >>= 1) {
-      kmodel += __shfl_xor_sync(0xffffffffu, kmodel, o);
-      kexec += __shfl_xor_sync(0xffffffffu, kexec, o);
+      km64 += __shfl_xor_sync(0xffffffffu, km64, o);
+      ke64 += __shfl_xor_sync(0xffffffffu, ke64, o);
+      km32 += __shfl_xor_sync(0xffffffffu, km32, o);
+      ke32 += __shfl_xor_sync(0xffffffffu, ke32, o);
     }
     if (lane == 0) {
-      cnt[warp] = c;
-      if (c) {
-        atomicAdd(blkacc + 2 * blk, kmodel * (unsigned long long)P.kk[bra]);
-        atomicAdd(blkacc + 2 * blk + 1, kexec * (unsigned long long)P.np[bra]);
+      cnt[warp] = c64;
+      cnt[ntask + warp] = c32;
+      if (c64) {
+        atomicAdd(blkacc + 4 * blk + 0, km64 * (unsigned long long)P.kk[bra]);
+        atomicAdd(blkacc + 4 * blk + 1, ke64 * (unsigned long long)P.np[bra]);
+      }
+      if (c32) {
+        atomicAdd(blkacc + 4 * blk + 2, km32 * (unsigned long long)P.kk[bra]);
+        atomicAdd(blkacc + 4 * blk + 3, ke32 * (unsigned long long)P.np[bra]);
       }
     }
   }
 }
 
-// block ranges [beg, end) of the quartet list from the per-task counts and offsets
-__global__ void k_block_ranges(BlockTable bt, const long long *__restrict__ cnt, const long long *__restrict__ off,
-                               long long *__restrict__ range) {
-  int b = threadIdx.x;
-  if (b >= bt.nblk) return;
-  int t0 = bt.task_beg[b], t1 = bt.task_beg[b + 1];
+// Ranges [beg, end) of the quartet list per (precision, class block) from the per-task
+// counts and offsets; virtual block b = prec * nblk + block, prec 0 = FP64, 1 = FP32.
+__global__ void k_block_ranges(BlockTable bt, int ntask, const long long *__restrict__ cnt,
+                               const long long *__restrict__ off, long long *__restrict__ range) {
+  int vb = threadIdx.x;
+  if (vb >= 2 * bt.nblk) return;
+  const int prec = vb / bt.nblk, b = vb % bt.nblk;
+  const int t0 = prec * ntask + bt.task_beg[b], t1 = prec * ntask + bt.task_beg[b + 1];
   long long beg = 0, end = 0;
   if (t1 > t0) {
     beg = off[t0];
@@ -275,8 +297,8 @@ __global__ void k_block_ranges(BlockTable bt, const long long *__restrict__ cnt,
   } else if (t0 > 0) {
     beg = end = off[t0 - 1] + cnt[t0 - 1];
   }
-  range[2 * b] = beg;
-  range[2 * b + 1] = end;
+  range[2 * vb] = beg;
+  range[2 * vb + 1] = end;
 }
 
 __device__ __forceinline__ double warp_sum(double x) {
@@ -404,14 +426,15 @@ __device__ __forceinline__ void digest(const double *v, double deg, int a0, int 
   }
 }
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, typename T>
 __device__ __forceinline__ void eri_jk_one(const uint2 *__restrict__ ql, long long i, long long wfirst, long long end,
                                            const Pairs &P, const Shells &S, const double *boys,
                                            const DigestGroups &dg);
 
 // Per-thread class kernel: persistent grid over the class's quartet range; the Boys rows
-// of this class are staged in shared memory once per block.
-template <int LA, int LB, int LC, int LD>
+// of this class are staged in shared memory once per block.  T is the arithmetic type of
+// everything after the (FP64) Boys values; the digest accumulates in FP64.
+template <int LA, int LB, int LC, int LD, typename T>
 __global__ void __launch_bounds__(128) k_eri_jk(const uint2 *__restrict__ ql, const long long *__restrict__ range,
                                                 int blk, Pairs P, Shells S, const double *__restrict__ boys_g,
                                                 DigestGroups dg) {
@@ -423,11 +446,11 @@ __global__ void __launch_bounds__(128) k_eri_jk(const uint2 *__restrict__ ql, co
   for (long long i = beg + blockIdx.x * (long long)blockDim.x + threadIdx.x;; i += stride) {
     const long long wfirst = i - (threadIdx.x & 31);
     if (wfirst >= end) return;   // the whole warp is past the end of the class
-    eri_jk_one<LA, LB, LC, LD>(ql, i, wfirst, end, P, S, boys, dg);
+    eri_jk_one<LA, LB, LC, LD, T>(ql, i, wfirst, end, P, S, boys, dg);
   }
 }
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, typename T>
 __device__ __forceinline__ void eri_jk_one(const uint2 *__restrict__ ql, long long i, long long wfirst, long long end,
                                            const Pairs &P, const Shells &S, const double *boys,
                                            const DigestGroups &dg) {
@@ -438,8 +461,16 @@ __device__ __forceinline__ void eri_jk_one(const uint2 *__restrict__ ql, long lo
   double v[NA * NB * NC * ND];
   if (valid) {
     const double3 A = S.center[ab.x], B = S.center[ab.y], C = S.center[cd.x], D = S.center[cd.y];
-    EriClass<LA, LB, LC, LD>::template run<double>(P.prim + P.poff[e.x], P.np[e.x], P.prim + P.poff[e.y],
-                                                   P.np[e.y], A, B, C, D, boys, v);
+    if constexpr (sizeof(T) == sizeof(double)) {
+      EriClass<LA, LB, LC, LD>::template run<double>(P.prim + P.poff[e.x], P.np[e.x], P.prim + P.poff[e.y],
+                                                     P.np[e.y], A, B, C, D, boys, v);
+    } else {
+      T vt[NA * NB * NC * ND];
+      EriClass<LA, LB, LC, LD>::template run<T>(P.prim + P.poff[e.x], P.np[e.x], P.prim + P.poff[e.y], P.np[e.y],
+                                                A, B, C, D, boys, vt);
+#pragma unroll
+      for (int k = 0; k < NA * NB * NC * ND; ++k) v[k] = (double)vt[k];
+    }
   } else {
 #pragma unroll
     for (int k = 0; k < NA * NB * NC * ND; ++k) v[k] = 0.0;
@@ -453,7 +484,7 @@ __device__ __forceinline__ void eri_jk_one(const uint2 *__restrict__ ql, long lo
 // ------------------------------------------------------------- warp-mode classes ---
 // SCHWARZ = false: quartets from the list, J/K digest.  SCHWARZ = true: "quartet" i is
 // pair i with itself, and the kernel writes Q(i) = sqrt(max |(ab|ab)| diagonal).
-template <int LA, int LB, int LC, int LD, bool SCHWARZ>
+template <int LA, int LB, int LC, int LD, bool SCHWARZ, typename T>
 __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ ql, const long long *__restrict__ range,
                                                      int blk, long long sbeg, long long send, Pairs P, Shells S,
                                                      const double *__restrict__ boys, DigestGroups dg,
@@ -486,13 +517,16 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  double *Eb = smem + (size_t)wid * (3 * WD::NEB + 3 * WD::NEK + 2 * WD::HL + 2 * NBUF + WD::NXS);
-  double *Ek = Eb + 3 * WD::NEB;
-  double *Ra = Ek + 3 * WD::NEK;
-  double *Rb = Ra + WD::HL;
-  double *W = Rb + WD::HL;
-  double *Cc = W + NBUF;
-  double *Xs = Cc + NBUF;   // staged density blocks for the digest
+  // per warp: staged density blocks (double) then the T work arrays
+  constexpr size_t WARP_BYTES = sizeof(double) * WD::NXS + sizeof(T) * (3 * WD::NEB + 3 * WD::NEK + 2 * WD::HL + 2 * NBUF);
+  constexpr size_t WARP_STRIDE = (WARP_BYTES + 15) / 16 * 16;
+  double *Xs = reinterpret_cast<double *>(reinterpret_cast<char *>(smem) + wid * WARP_STRIDE);
+  T *Eb = reinterpret_cast<T *>(Xs + WD::NXS);
+  T *Ek = Eb + 3 * WD::NEB;
+  T *Ra = Ek + 3 * WD::NEK;
+  T *Rb = Ra + WD::HL;
+  T *W = Rb + WD::HL;
+  T *Cc = W + NBUF;
   long long beg, end;
   if (SCHWARZ) {
     beg = sbeg;
@@ -512,7 +546,7 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
     const PrimPair *pkp = P.prim + P.poff[e.y];
     const int nb = P.np[e.x], nk = P.np[e.y];
     __syncwarp();
-    for (int k = lane; k < WD::NC; k += 32) Cc[k] = 0.0;
+    for (int k = lane; k < WD::NC; k += 32) Cc[k] = T(0);
     for (int ib = 0; ib < nb; ++ib) {
       const PrimPair bp = pbp[ib];
       __syncwarp();
@@ -520,9 +554,9 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
         const double Pc = lane == 0 ? bp.Px : (lane == 1 ? bp.Py : bp.Pz);
         const double Ac = lane == 0 ? A.x : (lane == 1 ? A.y : A.z);
         const double Bc = lane == 0 ? B.x : (lane == 1 ? B.y : B.z);
-        warpmd::build_E1<LA, LB, double>(Eb + lane * WD::NEB, Pc - Ac, Pc - Bc, 0.5 * bp.ip);
+        warpmd::build_E1<LA, LB, T>(Eb + lane * WD::NEB, T(Pc - Ac), T(Pc - Bc), T(0.5 * bp.ip));
       }
-      for (int k = lane; k < WD::NW; k += 32) W[k] = 0.0;
+      for (int k = lane; k < WD::NW; k += 32) W[k] = T(0);
       for (int ik = 0; ik < nk; ++ik) {
         const PrimPair kp = pkp[ik];
         __syncwarp();
@@ -530,7 +564,7 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
           const double Pc = lane == 0 ? kp.Px : (lane == 1 ? kp.Py : kp.Pz);
           const double Cc3 = lane == 0 ? C.x : (lane == 1 ? C.y : C.z);
           const double Dc = lane == 0 ? D.x : (lane == 1 ? D.y : D.z);
-          warpmd::build_E1<LC, LD, double>(Ek + lane * WD::NEK, Pc - Cc3, Pc - Dc, 0.5 * kp.ip);
+          warpmd::build_E1<LC, LD, T>(Ek + lane * WD::NEK, T(Pc - Cc3), T(Pc - Dc), T(0.5 * kp.ip));
         }
         const double pq = bp.p + kp.p;
         const double rpq = rsqrt(pq);
@@ -549,40 +583,41 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
           }
         }
         // R^{(n)}_{tuv}, n = L .. 0, ping-pong between Ra and Rb; level L in Ra when L even
-        double *prev = (L % 2 == 0) ? Rb : Ra;
-        double *cur = (L % 2 == 0) ? Ra : Rb;
+        T *prev = (L % 2 == 0) ? Rb : Ra;
+        T *cur = (L % 2 == 0) ? Ra : Rb;
+        const T Xt = T(X), Yt = T(Y), Zt = T(Z);
         // level L: one entry
-        if (lane == 0) cur[0] = fac[L];
+        if (lane == 0) cur[0] = T(fac[L]);
 #pragma unroll 1
         for (int n = L - 1; n >= 0; --n) {
-          double *t_ = prev;
+          T *t_ = prev;
           prev = cur;
           cur = t_;
           __syncwarp();
           const int cnt = warpmd::nherm(L - n);
           for (int h = lane; h < cnt; h += 32) {
-            double val;
+            T val;
             if (h == 0) {
-              val = fac[n];
+              val = T(fac[n]);
             } else {
               const int hc = s_h[h];
               const int t = hc & 15, u = (hc >> 4) & 15, v = hc >> 8;
               if (t > 0) {
-                val = X * prev[warpmd::hidx(t - 1, u, v)];
-                if (t > 1) val += (t - 1) * prev[warpmd::hidx(t - 2, u, v)];
+                val = Xt * prev[warpmd::hidx(t - 1, u, v)];
+                if (t > 1) val += T(t - 1) * prev[warpmd::hidx(t - 2, u, v)];
               } else if (u > 0) {
-                val = Y * prev[warpmd::hidx(t, u - 1, v)];
-                if (u > 1) val += (u - 1) * prev[warpmd::hidx(t, u - 2, v)];
+                val = Yt * prev[warpmd::hidx(t, u - 1, v)];
+                if (u > 1) val += T(u - 1) * prev[warpmd::hidx(t, u - 2, v)];
               } else {
-                val = Z * prev[warpmd::hidx(t, u, v - 1)];
-                if (v > 1) val += (v - 1) * prev[warpmd::hidx(t, u, v - 2)];
+                val = Zt * prev[warpmd::hidx(t, u, v - 1)];
+                if (v > 1) val += T(v - 1) * prev[warpmd::hidx(t, u, v - 2)];
               }
             }
             cur[h] = val;
           }
         }
         __syncwarp();
-        const double *R = cur;  // level 0
+        const T *R = cur;  // level 0
         // W[tuv][cd] += sum (-1)^(tau+nu+phi) E^cd R
         for (int e2 = lane; e2 < WD::NW; e2 += 32) {
           const int h = e2 / NCCD, c = e2 % NCCD;
@@ -591,15 +626,15 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
           const int cx = cc & 15, cy = (cc >> 4) & 15, cz = (cc >> 8) & 15;
           const int dx = (cc >> 12) & 15, dy = (cc >> 16) & 15, dz = cc >> 20;
           constexpr int NT = WD::Q + 1;
-          const double *ex = Ek + (cx * (LD + 1) + dx) * NT;
-          const double *ey = Ek + WD::NEK + (cy * (LD + 1) + dy) * NT;
-          const double *ez = Ek + 2 * WD::NEK + (cz * (LD + 1) + dz) * NT;
-          double s = 0.0;
+          const T *ex = Ek + (cx * (LD + 1) + dx) * NT;
+          const T *ey = Ek + WD::NEK + (cy * (LD + 1) + dy) * NT;
+          const T *ez = Ek + 2 * WD::NEK + (cz * (LD + 1) + dz) * NT;
+          T s = T(0);
           for (int a1 = 0; a1 <= cx + dx; ++a1)
             for (int a2 = 0; a2 <= cy + dy; ++a2) {
-              const double exy = ((a1 + a2) & 1 ? -1.0 : 1.0) * ex[a1] * ey[a2];
+              const T exy = ((a1 + a2) & 1 ? T(-1) : T(1)) * ex[a1] * ey[a2];
               for (int a3 = 0; a3 <= cz + dz; ++a3) {
-                const double c3 = (a3 & 1) ? -ez[a3] : ez[a3];
+                const T c3 = (a3 & 1) ? -ez[a3] : ez[a3];
                 s += exy * c3 * R[warpmd::hidx(t + a1, u + a2, v + a3)];
               }
             }
@@ -614,13 +649,13 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
         const int ax = cc & 15, ay = (cc >> 4) & 15, az = (cc >> 8) & 15;
         const int bx = (cc >> 12) & 15, by = (cc >> 16) & 15, bz = cc >> 20;
         constexpr int NT = WD::P + 1;
-        const double *ex = Eb + (ax * (LB + 1) + bx) * NT;
-        const double *ey = Eb + WD::NEB + (ay * (LB + 1) + by) * NT;
-        const double *ez = Eb + 2 * WD::NEB + (az * (LB + 1) + bz) * NT;
-        double s = 0.0;
+        const T *ex = Eb + (ax * (LB + 1) + bx) * NT;
+        const T *ey = Eb + WD::NEB + (ay * (LB + 1) + by) * NT;
+        const T *ez = Eb + 2 * WD::NEB + (az * (LB + 1) + bz) * NT;
+        T s = T(0);
         for (int a1 = 0; a1 <= ax + bx; ++a1)
           for (int a2 = 0; a2 <= ay + by; ++a2) {
-            const double exy = ex[a1] * ey[a2];
+            const T exy = ex[a1] * ey[a2];
             for (int a3 = 0; a3 <= az + bz; ++a3) s += exy * ez[a3] * W[warpmd::hidx(a1, a2, a3) * NCCD + c];
           }
         Cc[e2] += s;
@@ -628,7 +663,7 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
     }
     __syncwarp();
     // Cartesian -> spherical on pure axes (L > 1), ping-pong Cc <-> W
-    double *src = Cc, *dst = W;
+    T *src = Cc, *dst = W;
     {
       int d[4] = {warpmd::ncart(LA), warpmd::ncart(LB), warpmd::ncart(LC), warpmd::ncart(LD)};
       const int ls[4] = {LA, LB, LC, LD};
@@ -636,19 +671,19 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
       for (int ax = 0; ax < 4; ++ax) {
         if (ls[ax] < 2) continue;
         const double *Ct = ls[ax] == 2 ? kSph2 : kSph3;
-        warpmd::sph_axis<double>(src, dst, d, ax, ls[ax], Ct, lane);
+        warpmd::sph_axis<T>(src, dst, d, ax, ls[ax], Ct, lane);
         d[ax] = 2 * ls[ax] + 1;
-        double *t_ = src;
+        T *t_ = src;
         src = dst;
         dst = t_;
         __syncwarp();
       }
     }
-    const double *V = src;   // [a][b][c][d] in the reference basis
+    const T *V = src;   // [a][b][c][d] in the reference basis
     constexpr int NA = WD::NSA, NB = WD::NSB, NC = WD::NSC, ND = WD::NSD;
     if (SCHWARZ) {
       double mx = 0.0;
-      for (int k = lane; k < NA * NB; k += 32) mx = fmax(mx, fabs(V[k * (NA * NB) + k]));
+      for (int k = lane; k < NA * NB; k += 32) mx = fmax(mx, fabs((double)V[k * (NA * NB) + k]));
       for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
       if (lane == 0) Qout[q] = sqrt(mx);
       continue;
@@ -719,11 +754,12 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
   }
 }
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, typename T>
 static size_t warp_smem_bytes() {
   using WD = warpmd::WarpDims<LA, LB, LC, LD>;
   constexpr int NBUF = (WD::NW > WD::NC) ? WD::NW : WD::NC;
-  return sizeof(double) * 4 * (size_t)(3 * WD::NEB + 3 * WD::NEK + 2 * WD::HL + 2 * NBUF + WD::NXS);
+  constexpr size_t WARP_BYTES = sizeof(double) * WD::NXS + sizeof(T) * (3 * WD::NEB + 3 * WD::NEK + 2 * WD::HL + 2 * NBUF);
+  return 4 * ((WARP_BYTES + 15) / 16 * 16);
 }
 
 // AX += 0.5 (Gh + Gh^T)
@@ -867,22 +903,22 @@ __host__ __device__ constexpr bool is_warp_class(int la, int lb, int lc, int ld)
   return ncart_c(la) * ncart_c(lb) * ncart_c(lc) * ncart_c(ld) > 150;
 }
 
-template <int LA, int LB, int LC, int LD, bool SCHWARZ>
+template <int LA, int LB, int LC, int LD, bool SCHWARZ, typename T>
 static cudaError_t launch_warp(cqg_ctx *ctx, int blk, long long n, long long sbeg, long long send, cudaStream_t st,
                                const DigestGroups &dg, double *Q) {
   if (n <= 0) return cudaSuccess;
   static bool attr_set = false;
-  const size_t smem = warp_smem_bytes<LA, LB, LC, LD>();
+  const size_t smem = warp_smem_bytes<LA, LB, LC, LD, T>();
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(k_eri_jk_warp<LA, LB, LC, LD, SCHWARZ>,
+    cudaError_t e = cudaFuncSetAttribute(k_eri_jk_warp<LA, LB, LC, LD, SCHWARZ, T>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
   const int blocks = (int)std::min<long long>((n + 3) / 4, 148LL * 16);
-  k_eri_jk_warp<LA, LB, LC, LD, SCHWARZ><<<blocks, 128, smem, st>>>(ctx->d_qlist.p, ctx->d_range.p, blk, sbeg, send,
-                                                                    make_pairs(ctx), make_shells(ctx), ctx->d_boys.p,
-                                                                    dg, Q);
+  k_eri_jk_warp<LA, LB, LC, LD, SCHWARZ, T><<<blocks, 128, smem, st>>>(ctx->d_qlist.p, ctx->d_range.p, blk, sbeg,
+                                                                       send, make_pairs(ctx), make_shells(ctx),
+                                                                       ctx->d_boys.p, dg, Q);
   return cudaGetLastError();
 }
 
@@ -893,7 +929,7 @@ static cudaError_t launch_schwarz(cqg_ctx *ctx, Pairs P, Shells S, int beg, int 
   if constexpr (is_warp_class(LA, LB, LA, LB)) {
     DigestGroups dg;
     memset(&dg, 0, sizeof(dg));
-    return launch_warp<LA, LB, LA, LB, true>(ctx, 0, n, beg, end, 0, dg, Q);
+    return launch_warp<LA, LB, LA, LB, true, double>(ctx, 0, n, beg, end, 0, dg, Q);
   } else {
     k_schwarz<LA, LB><<<(n + 127) / 128, 128>>>(P, S, ctx->d_boys.p, beg, end, Q);
     return cudaGetLastError();
@@ -992,29 +1028,32 @@ static cqg_status upload_pairs(cqg_ctx *ctx, double prim_thresh) {
 
 typedef cudaError_t (*eri_launcher)(cqg_ctx *, int blk, long long n, cudaStream_t st, const DigestGroups &dg);
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, typename T>
 static cudaError_t launch_eri(cqg_ctx *ctx, int blk, long long n, cudaStream_t st, const DigestGroups &dg) {
   if (n <= 0) return cudaSuccess;
   if constexpr (is_warp_class(LA, LB, LC, LD)) {
-    return launch_warp<LA, LB, LC, LD, false>(ctx, blk, n, 0, 0, st, dg, nullptr);
+    return launch_warp<LA, LB, LC, LD, false, T>(ctx, blk, n, 0, 0, st, dg, nullptr);
   } else {
     long long nb = std::min<long long>((n + 127) / 128, 148LL * 12);
-    k_eri_jk<LA, LB, LC, LD><<<(unsigned)nb, 128, 0, st>>>(ctx->d_qlist.p, ctx->d_range.p, blk, make_pairs(ctx),
+    k_eri_jk<LA, LB, LC, LD, T><<<(unsigned)nb, 128, 0, st>>>(ctx->d_qlist.p, ctx->d_range.p, blk, make_pairs(ctx),
                                                            make_shells(ctx), ctx->d_boys.p, dg);
     return cudaGetLastError();
   }
 }
 
-#define QC(a, b, c, d) &launch_eri<a, b, c, d>
-static const eri_launcher kEriLaunch[CQG_NQC] = {
-    QC(0, 0, 0, 0),
-    QC(1, 0, 0, 0), QC(1, 0, 1, 0),
-    QC(1, 1, 0, 0), QC(1, 1, 1, 0), QC(1, 1, 1, 1),
-    QC(2, 0, 0, 0), QC(2, 0, 1, 0), QC(2, 0, 1, 1), QC(2, 0, 2, 0),
-    QC(2, 1, 0, 0), QC(2, 1, 1, 0), QC(2, 1, 1, 1), QC(2, 1, 2, 0), QC(2, 1, 2, 1),
-    QC(2, 2, 0, 0), QC(2, 2, 1, 0), QC(2, 2, 1, 1), QC(2, 2, 2, 0), QC(2, 2, 2, 1), QC(2, 2, 2, 2),
-};
+#define CLASS_TABLE(T)                                                                                   \
+  {QC(0, 0, 0, 0, T),                                                                                    \
+   QC(1, 0, 0, 0, T), QC(1, 0, 1, 0, T),                                                                 \
+   QC(1, 1, 0, 0, T), QC(1, 1, 1, 0, T), QC(1, 1, 1, 1, T),                                              \
+   QC(2, 0, 0, 0, T), QC(2, 0, 1, 0, T), QC(2, 0, 1, 1, T), QC(2, 0, 2, 0, T),                           \
+   QC(2, 1, 0, 0, T), QC(2, 1, 1, 0, T), QC(2, 1, 1, 1, T), QC(2, 1, 2, 0, T), QC(2, 1, 2, 1, T),        \
+   QC(2, 2, 0, 0, T), QC(2, 2, 1, 0, T), QC(2, 2, 1, 1, T), QC(2, 2, 2, 0, T), QC(2, 2, 2, 1, T),        \
+   QC(2, 2, 2, 2, T)}
+#define QC(a, b, c, d, T) &launch_eri<a, b, c, d, T>
+static const eri_launcher kEriLaunch[CQG_NQC] = CLASS_TABLE(double);
+static const eri_launcher kEriLaunch32[CQG_NQC] = CLASS_TABLE(float);
 #undef QC
+#undef CLASS_TABLE
 
 extern "C" {
 
@@ -1277,10 +1316,10 @@ cqg_status cqg_set_basis(cqg_ctx *ctx, int nshell, const int *L, const int *pure
   bt.nblk = CQG_NQC;
   ctx->ntask = task;
   size_t scan_bytes = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (long long *)nullptr, (long long *)nullptr, std::max(task, 1));
-  if (ctx->d_cnt.reserve(task + 1) || ctx->d_off.reserve(task + 1) || ctx->d_range.reserve(2 * CQG_NQC) ||
+  cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (long long *)nullptr, (long long *)nullptr, std::max(2 * task, 1));
+  if (ctx->d_cnt.reserve(2 * task + 1) || ctx->d_off.reserve(2 * task + 1) || ctx->d_range.reserve(4 * CQG_NQC) ||
       ctx->d_scan_tmp.reserve(scan_bytes + 16) || ctx->d_M.reserve((size_t)nshell * nshell) ||
-      ctx->d_Mmax.reserve(1) || ctx->d_flags.reserve(4) || ctx->d_blkacc.reserve(2 * CQG_NQC))
+      ctx->d_Mmax.reserve(1) || ctx->d_flags.reserve(4) || ctx->d_blkacc.reserve(4 * CQG_NQC))
     return CQG_ERR_OOM;
   return CQG_OK;
 }
@@ -1303,7 +1342,8 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
   for (int i = 0; i < nx_all; ++i) xl.X[i] = Xall[i];
   CUCHK(cudaMemsetAsync(ctx->d_flags.p, 0, 4 * sizeof(int), st));
   CUCHK(cudaMemsetAsync(ctx->d_Mmax.p, 0, sizeof(double), st));
-  CUCHK(cudaMemsetAsync(ctx->d_blkacc.p, 0, 2 * CQG_NQC * sizeof(unsigned long long), st));
+  CUCHK(cudaMemsetAsync(ctx->d_blkacc.p, 0, 4 * CQG_NQC * sizeof(unsigned long long), st));
+  const double cut32 = ctx->policy == CQG_PREC_MIXED ? ctx->fp32_cutoff : 0.0;
   ctx->launches = 0;
   {
     dim3 g((nsh + 127) / 128, nsh);
@@ -1321,16 +1361,16 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     int nthr = 256, wpb = nthr / 32;
     int nb = (ctx->ntask + wpb - 1) / wpb;
     k_quartets<false><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, nsh, ctx->d_Mmax.p, ctx->thresh,
-                                            ctx->d_cnt.p, nullptr, nullptr, ctx->d_blkacc.p);
+                                            cut32, ctx->d_cnt.p, nullptr, nullptr, ctx->d_blkacc.p);
     CUCHK(cudaGetLastError());
     size_t scan_bytes = ctx->d_scan_tmp.n;
-    CUCHK(cub::DeviceScan::ExclusiveSum(ctx->d_scan_tmp.p, scan_bytes, ctx->d_cnt.p, ctx->d_off.p, ctx->ntask, st));
-    k_block_ranges<<<1, 64, 0, st>>>(ctx->bt, ctx->d_cnt.p, ctx->d_off.p, ctx->d_range.p);
+    CUCHK(cub::DeviceScan::ExclusiveSum(ctx->d_scan_tmp.p, scan_bytes, ctx->d_cnt.p, ctx->d_off.p, 2 * ctx->ntask, st));
+    k_block_ranges<<<1, 128, 0, st>>>(ctx->bt, ctx->ntask, ctx->d_cnt.p, ctx->d_off.p, ctx->d_range.p);
     CUCHK(cudaGetLastError());
     ctx->launches += 2;
   }
-  long long hr[2 * CQG_NQC];
-  unsigned long long hacc[2 * CQG_NQC];
+  long long hr[4 * CQG_NQC];
+  unsigned long long hacc[4 * CQG_NQC];
   int hflags[4];
   CUCHK(cudaMemcpyAsync(hr, ctx->d_range.p, sizeof(hr), cudaMemcpyDeviceToHost, st));
   CUCHK(cudaMemcpyAsync(hacc, ctx->d_blkacc.p, sizeof(hacc), cudaMemcpyDeviceToHost, st));
@@ -1344,7 +1384,7 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     ctx->err = "input matrix is not symmetric; this engine contracts real symmetric X only";
     return CQG_ERR_UNSUPPORTED;
   }
-  long long total = hr[2 * CQG_NQC - 1];
+  long long total = hr[4 * CQG_NQC - 1];
   if (ctx->d_qlist.reserve((size_t)std::max<long long>(total, 1)) != cudaSuccess) {
     ctx->err = "quartet list allocation failed";
     return CQG_ERR_OOM;
@@ -1353,7 +1393,7 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     int nthr = 256, wpb = nthr / 32;
     int nb = (ctx->ntask + wpb - 1) / wpb;
     k_quartets<true><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, nsh, ctx->d_Mmax.p, ctx->thresh,
-                                           nullptr, ctx->d_off.p, ctx->d_qlist.p, nullptr);
+                                           cut32, nullptr, ctx->d_off.p, ctx->d_qlist.p, nullptr);
     CUCHK(cudaGetLastError());
     ctx->launches += 1;
   }
@@ -1374,19 +1414,25 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
   }
   memset(ctx->stats.class_quartets, 0, sizeof(ctx->stats.class_quartets));
   memset(ctx->stats.class_ms, 0, sizeof(ctx->stats.class_ms));
-  double mflops = 0;
-  long long nprimq = 0;
+  double mflops = 0, mflops32 = 0;
+  long long nprimq = 0, nq32 = 0;
   for (int k = 0; k < CQG_NQC; ++k) {
-    long long nq = hr[2 * k + 1] - hr[2 * k];
-    ctx->stats.class_quartets[k] = nq;
+    const long long n64 = hr[2 * k + 1] - hr[2 * k];
+    const long long n32 = hr[2 * (CQG_NQC + k) + 1] - hr[2 * (CQG_NQC + k)];
+    ctx->stats.class_quartets[k] = n64 + n32;
+    nq32 += n32;
     int i, j;
     qclass_split(k, i, j);
     const int la = kPairClass[i][0], lb = kPairClass[i][1], lc = kPairClass[j][0], ld = kPairClass[j][1];
-    mflops += (double)hacc[2 * k] * md_v1_prim_flops(la, lb, lc, ld) + (double)nq * md_v1_digest_flops(la, lb, lc, ld);
-    nprimq += (long long)hacc[2 * k + 1];
-    if (nq > 0) ctx->launches += 1;
+    const double fp = md_v1_prim_flops(la, lb, lc, ld), fd = md_v1_digest_flops(la, lb, lc, ld);
+    mflops += (double)hacc[4 * k] * fp + (double)n64 * fd;
+    mflops32 += (double)hacc[4 * k + 2] * fp + (double)n32 * fd;
+    nprimq += (long long)(hacc[4 * k + 1] + hacc[4 * k + 3]);
+    if (n64 > 0) ctx->launches += 1;
+    if (n32 > 0) ctx->launches += 1;
     if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[4 + 2 * k], st));
-    cudaError_t e = kEriLaunch[k](ctx, k, nq, st, dg);
+    cudaError_t e = kEriLaunch[k](ctx, k, n64, st, dg);
+    if (e == cudaSuccess) e = kEriLaunch32[k](ctx, CQG_NQC + k, n32, st, dg);
     if (e != cudaSuccess) {
       ctx->err = std::string("eri kernel ") + cqg_class_name(k) + ": " + cudaGetErrorString(e);
       return CQG_ERR_CUDA;
@@ -1403,8 +1449,9 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
   }
   if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[3], st));
   ctx->stats.quartets = total;
-  ctx->stats.quartets_fp32 = 0;
-  ctx->stats.model_flops = mflops;
+  ctx->stats.quartets_fp32 = nq32;
+  ctx->stats.model_flops = mflops + mflops32;
+  ctx->stats.model_flops_fp32 = mflops32;
   ctx->stats.prim_quartets = nprimq;
   ctx->stats.launches = ctx->launches;
   return CQG_OK;

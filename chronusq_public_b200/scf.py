@@ -91,6 +91,12 @@ class SingleSlater:
         self.dampParam = 0.1
         self.xHF = -0.5
         self.guess = "SAD"
+        # mixed precision + incremental (Delta D) Fock build
+        self.precision = "fp64"        # "fp64" or "mixed"
+        self.fp32_cutoff = 1e-8        # density-weighted Schwarz bound below which a quartet runs in FP32
+        self.incremental = False       # build PT_k = PT_{k-1} + G[D_k - D_{k-1}]
+        self.nIncFock = 20             # full rebuild period of the incremental build (singleslater.h:468)
+        self.fp64_switch = 1e-5        # DIIS error below which the builds return to full FP64
         self.n = basis.nbasis
         self.log: List[SCFIteration] = []
         self.fock_builds = 0
@@ -108,6 +114,13 @@ class SingleSlater:
         self.Enuc = self.mol.nuclear_repulsion()
 
     # ------------------------------------------------------------------ pieces ---
+    def _set_precision(self, mixed: bool):
+        from .aointegrals import PREC_FP64, PREC_MIXED
+        if mixed:
+            self.ints.setPrecision(PREC_MIXED, self.fp32_cutoff)
+        else:
+            self.ints.setPrecision(PREC_FP64, 0.0)
+
     def formPT(self, Ps, Pz=None):
         t0 = time.perf_counter()
         PTs, PTz = self.ints.formPT(Ps, None if self.isClosedShell else Pz, xHF=self.xHF)
@@ -205,6 +218,7 @@ class SingleSlater:
         t.cuda.synchronize(self.dev)
         t0 = time.perf_counter()
         self.log = []
+        self._set_precision(self.precision == "mixed")
         Ps, Pz, FOs_prev, FOz_prev = self.formGuess(density)
         Eold = 0.0
         self.converged = False
@@ -212,8 +226,26 @@ class SingleSlater:
         diis_on = self.doDIIS
         damp = self.dampParam if self.doDamp else 0.0
         xsmall = np.finfo(float).eps * 10 * 5
+        mixed_phase = self.precision == "mixed"
+        self._set_precision(mixed_phase)
+        built = None            # (Ps, Pz, PTs, PTz) of the last build, for Delta D
+        since_full = 0
+        self.phase_switch_iter = None
+        self.fp32_quartets = 0
         for it in range(self.maxSCFIter):
-            Fs, Fz, PTs, PTz = self.formFock(Ps, Pz)
+            if self.incremental and built is not None and since_full < self.nIncFock:
+                dPs, dPz = Ps - built[0], Pz - built[1]
+                dPTs, dPTz = self.formPT(dPs, dPz)
+                PTs, PTz = built[2] + dPTs, built[3] + dPTz
+                since_full += 1
+            else:
+                PTs, PTz = self.formPT(Ps, Pz)
+                since_full = 0
+            if mixed_phase:
+                self.fp32_quartets += self.ints.stats()["quartets_fp32"]
+            built = (Ps, Pz, PTs, PTz)
+            Fs = 2.0 * self.coreH + PTs
+            Fz = PTz.clone()
             FOs, FOz = self._ortho(Fs), self._ortho(Fz)
             DOs = self.X.T @ self.overlap @ Ps @ self.overlap @ self.X   # orthonormal density
             DOz = self.X.T @ self.overlap @ Pz @ self.overlap @ self.X
@@ -226,6 +258,12 @@ class SingleSlater:
                 errs = [ea - ea.T, eb - eb.T]
             cnorm = max(float(t.linalg.norm(e)) for e in errs)
             fp_converged = cnorm < xsmall
+            if mixed_phase and cnorm < self.fp64_switch:
+                # last iterations in FP64, starting from a full rebuild
+                mixed_phase = False
+                self._set_precision(False)
+                self.phase_switch_iter = it
+                built = None
             if diis_on:
                 hist_F.append((Fs, Fz))
                 hist_PT.append((PTs, PTz))

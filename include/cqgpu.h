@@ -54,6 +54,7 @@ typedef struct {
   long long quartets_fp32;         /* of which evaluated in FP32 (mixed policy) */
   long long prim_quartets;         /* primitive quartets evaluated */
   double model_flops;              /* MD-v1 model FLOPs of the screened quartets */
+  double model_flops_fp32;         /* of which in FP32 quartets */
   double ms_screen;                /* device time of screening + list build (ms) */
   double ms_eri;                   /* device time of ERI + digest kernels (ms) */
   double ms_total;                 /* device time of the whole call (ms) */

@@ -1,0 +1,53 @@
+"""Mixed-precision (FP32 quartets below a Schwarz-bound cutoff, FP64 accumulation) and
+incremental Delta-D Fock builds against the all-FP64 GPU build."""
+import numpy as np
+import pytest
+
+from chronusq_public_b200.basis import BasisSet
+from chronusq_public_b200.molecule import water_cluster
+
+pytestmark = pytest.mark.gpu
+
+
+def _rand_density(n, seed):
+    rng = np.random.default_rng(seed)
+    a = rng.uniform(-1, 1, (n, n))
+    return np.asfortranarray(0.5 * (a + a.T))
+
+
+@pytest.mark.parametrize("cutoff", [1e-10, 1e-8, 1e-6])
+def test_mixed_G_close_to_fp64(cutoff):
+    from chronusq_public_b200.aointegrals import AOIntegrals, PREC_MIXED, PREC_FP64
+    mol = water_cluster(4, 21)
+    bs = BasisSet("cc-pvdz", mol.atoms, mol.coords)
+    ints = AOIntegrals(bs)
+    D = _rand_density(bs.nbasis, 4)
+    G64, _ = ints.formPT(D)
+    n64 = ints.stats()["quartets"]
+    ints.setPrecision(PREC_MIXED, cutoff)
+    G32, _ = ints.formPT(D)
+    st = ints.stats()
+    assert st["quartets"] == n64                 # same quartet set, split by precision
+    assert st["quartets_fp32"] > 0
+    err = np.abs(G32 - G64).max()
+    assert err < 50 * cutoff, err               # FP32 quartets are bounded by the cutoff
+    ints.setPrecision(PREC_FP64, 0.0)
+    G64b, _ = ints.formPT(D)
+    assert np.abs(G64b - G64).max() < 1e-12
+
+
+def test_mixed_incremental_scf_energy_within_1uEh():
+    from chronusq_public_b200.scf import SingleSlater
+    mol = water_cluster(3, 2)
+    bs = BasisSet("cc-pvdz", mol.atoms, mol.coords)
+    ref = SingleSlater(mol, bs)
+    E64 = ref.SCF3()
+    mx = SingleSlater(mol, bs, ints=ref.ints)
+    mx.precision = "mixed"
+    mx.fp32_cutoff = 1e-7
+    mx.incremental = True
+    E = mx.SCF3()
+    assert mx.fp32_quartets > 0
+    assert abs(E - E64) < 1e-6, (E, E64)
+    assert mx.time_to(E64, 1e-6) is not None
+    ref.close()
