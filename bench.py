@@ -4,9 +4,11 @@
 Workload (default): RHF Fock build G[D] = 2J[D] - K[D] (``formPT``, reference
 include/singleslater/singleslater_fock.h:31-93 -> newTwoEContractDirect) for a seeded
 (H2O)_32 cluster at liquid density in cc-pVDZ (768 basis functions, quartet classes up to
-(dd|dd)), Schwarz threshold 1e-14 (the reference default, include/aointegrals.h:334).
-One step = one Fock build over one density.  Metric: screened unique shell quartets per
-second (the reference's loop unit, contract.h:96-131).
+(dd|dd)), Schwarz threshold 1e-14 (the reference default, include/aointegrals.h:334), on
+the SAD-guess density.  One step = one Fock build over one density.  Metric: screened
+unique shell quartets per second (the reference's loop unit, contract.h:96-131).  The line
+also carries the time to a converged SCF (|dE| <= 1 uEh) of the plain FP64 build and of
+the mixed-precision incremental build.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -54,13 +56,24 @@ def synthetic_density(bs, seed):
     return np.ascontiguousarray(D)
 
 
-def build_workload(name):
+def build_workload(name, density="sad"):
+    """Molecule, basis and the density of the benchmarked Fock build: the SAD-guess
+    density of the SCF (atomic UHF densities, one Fock build, diagonalised; computed on
+    the GPU) or, with density="synthetic", a seeded distance-decaying matrix."""
     from chronusq_public_b200.basis import BasisSet
     from chronusq_public_b200.molecule import water_cluster, single_water
     w = WORKLOADS[name]
     mol = single_water(w["seed"]) if w["nwater"] == 1 else water_cluster(w["nwater"], w["seed"])
     bs = BasisSet(w["basis"], mol.atoms, mol.coords)
-    D = synthetic_density(bs, 1234)
+    if density == "synthetic":
+        D = synthetic_density(bs, 1234)
+    else:
+        from chronusq_public_b200.scf import SingleSlater
+        hf = SingleSlater(mol, bs, thresholdSchwartz=w["thresh"])
+        Ps, _, _, _ = hf.formGuess()
+        D = np.ascontiguousarray(Ps.cpu().numpy())
+        D = 0.5 * (D + D.T)
+        hf.close()
     return w, mol, bs, D
 
 
@@ -156,7 +169,7 @@ def cpu_baseline(bs, D, thresh, target_s=15.0, nthreads=0):
 def run_reference(args, ws, rank):
     if rank != 0:
         return
-    w, mol, bs, D = build_workload(args.workload)
+    w, mol, bs, D = build_workload(args.workload, args.density)
     base = cpu_baseline(bs, D, w["thresh"], target_s=args.ref_seconds)
     from oracle import oracle as O
     ob = O.OracleBasis.from_basis(bs)
@@ -191,8 +204,41 @@ def run_reference(args, ws, rank):
 def config_of(args, w, bs):
     return {"workload": args.workload, "molecule": "(H2O)_%d" % w["nwater"], "basis": w["basis"],
             "nbasis": bs.nbasis, "nshell": bs.nshell, "schwarz_threshold": w["thresh"],
-            "density": "seeded synthetic, distance-decaying", "l2": "flushed between steps (256 MiB write)",
+            "density": ("SAD guess density (GPU SCF guess path)" if args.density == "sad"
+                        else "seeded synthetic, distance-decaying"),
+            "geometry": "seeded water cluster at 1.0 g/cm^3 (Poisson-disk O centres, min O-O 2.6 A)",
+            "l2": "flushed between steps (256 MiB write)",
             "precision": "fp64", "parallelism": "replicas" if args.gpus > 1 else "single"}
+
+
+def scf_compare(mol, bs, thresh, cutoff, sweep=()):
+    """Time to converged SCF: plain FP64 GPU build vs mixed precision + incremental build.
+    Times include the SAD guess (atomic SCFs cached beforehand) and every iteration."""
+    from chronusq_public_b200.scf import SingleSlater
+    warm = SingleSlater(mol, bs, thresholdSchwartz=thresh)
+    warm.formGuess()                      # atomic SAD densities cached, kernels warm
+    plain = SingleSlater(mol, bs, ints=warm.ints)
+    E64 = plain.SCF3()
+    out = {"plain_fp64": {"energy": E64, "iterations": plain.nSCFIter, "seconds": plain.scf_seconds,
+                          "seconds_to_1uEh": plain.time_to(E64, 1e-6), "fock_builds": plain.fock_builds,
+                          "fock_seconds": plain.fock_seconds}}
+    runs = {}
+    for c in sorted(set([cutoff] + list(sweep))):
+        mx = SingleSlater(mol, bs, ints=warm.ints)
+        mx.precision, mx.fp32_cutoff, mx.incremental = "mixed", c, True
+        E = mx.SCF3()
+        runs["%.0e" % c] = {"energy": E, "abs_dE_vs_fp64": abs(E - E64), "iterations": mx.nSCFIter,
+                            "seconds": mx.scf_seconds, "seconds_to_1uEh": mx.time_to(E64, 1e-6),
+                            "fp32_quartets": mx.fp32_quartets, "fp64_switch_iteration": mx.phase_switch_iter}
+    out["mixed_incremental"] = runs["%.0e" % cutoff]
+    out["mixed_incremental"]["fp32_cutoff"] = cutoff
+    if sweep:
+        out["cutoff_sweep"] = runs
+    t_plain, t_mixed = out["plain_fp64"]["seconds_to_1uEh"], out["mixed_incremental"]["seconds_to_1uEh"]
+    if t_plain and t_mixed:
+        out["speedup_time_to_1uEh"] = t_plain / t_mixed
+    warm.close()
+    return out
 
 
 def main():
@@ -205,6 +251,10 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--class-table", action="store_true", help="print per-class times to stderr")
+    ap.add_argument("--density", default="sad", choices=["sad", "synthetic"])
+    ap.add_argument("--no-scf", action="store_true", help="skip the time-to-converged-SCF comparison")
+    ap.add_argument("--fp32-cutoff", type=float, default=1e-8)
+    ap.add_argument("--sweep", action="store_true", help="also sweep the FP32 cutoff 1e-10..1e-6")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     if args.impl == "reference":
@@ -221,7 +271,7 @@ def main():
     from chronusq_public_b200.aointegrals import AOIntegrals, probe_fma_peak
     from chronusq_public_b200 import _lib
 
-    w, mol, bs, D = build_workload(args.workload)
+    w, mol, bs, D = build_workload(args.workload, args.density)
     n = bs.nbasis
     ints = AOIntegrals(bs, device=local, thresholdSchwartz=w["thresh"])
     Dd = torch.from_numpy(D).cuda()
@@ -315,6 +365,9 @@ def main():
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
+        if not args.no_scf:
+            line["scf"] = scf_compare(mol, bs, w["thresh"], args.fp32_cutoff,
+                                      sweep=(1e-10, 1e-9, 1e-8, 1e-7, 1e-6) if args.sweep else ())
         if not args.no_cpu_baseline and ws == 1:
             line["cpu_baseline"] = cpu_baseline(bs, D, w["thresh"], target_s=args.ref_seconds)
         print(json.dumps(line), flush=True)

@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 GEN = os.path.join(CSRC, "_gen", "eri_classes.cuh")
 OUT = os.path.join(HERE, "libcqgpu.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
-MAXL = 2
+MAXL = 3
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-shared", "-Xcompiler", "-fPIC"]

@@ -29,15 +29,16 @@
 #include "eri_warp.cuh"
 #include "one_e.cuh"
 
-#define CQG_MAXL 2
+#define CQG_MAXL 3
 #define CQG_NPC ((CQG_MAXL + 1) * (CQG_MAXL + 2) / 2)       // pair classes
 #define CQG_NQC (CQG_NPC * (CQG_NPC + 1) / 2)                // quartet classes
 #define CQG_MAXG 4
-#define CQG_NBUCKET 8
+#define CQG_NBUCKET 16
 
 static_assert(CQG_NQC <= 55, "class table");
 
 // ------------------------------------------------------------------ class tables ---
+static_assert(CQG_GEN_MAXL == CQG_MAXL, "generated ERI code must match CQG_MAXL");
 static const int kPairClass[10][2] = {{0, 0}, {1, 0}, {1, 1}, {2, 0}, {2, 1}, {2, 2},
                                       {3, 0}, {3, 1}, {3, 2}, {3, 3}};
 static inline int pair_class_of(int la, int lb) {  // la >= lb
@@ -900,7 +901,7 @@ static Shells make_shells(cqg_ctx *ctx);
 
 // classes evaluated by the warp-cooperative kernel (same rule as gen_eri.WARP_CLASSES)
 __host__ __device__ constexpr bool is_warp_class(int la, int lb, int lc, int ld) {
-  return ncart_c(la) * ncart_c(lb) * ncart_c(lc) * ncart_c(ld) > 150;
+  return ncart_c(la) * ncart_c(lb) * ncart_c(lc) * ncart_c(ld) > 150 || la + lb + lc + ld >= 6;
 }
 
 template <int LA, int LB, int LC, int LD, bool SCHWARZ, typename T>
@@ -908,15 +909,17 @@ static cudaError_t launch_warp(cqg_ctx *ctx, int blk, long long n, long long sbe
                                const DigestGroups &dg, double *Q) {
   if (n <= 0) return cudaSuccess;
   static bool attr_set = false;
-  const size_t smem = warp_smem_bytes<LA, LB, LC, LD, T>();
+  const size_t per_warp = warp_smem_bytes<LA, LB, LC, LD, T>() / 4;
+  const int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (200u * 1024u) / per_warp));
+  const size_t smem = per_warp * wpb;
   if (!attr_set) {
     cudaError_t e = cudaFuncSetAttribute(k_eri_jk_warp<LA, LB, LC, LD, SCHWARZ, T>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
-  const int blocks = (int)std::min<long long>((n + 3) / 4, 148LL * 16);
-  k_eri_jk_warp<LA, LB, LC, LD, SCHWARZ, T><<<blocks, 128, smem, st>>>(ctx->d_qlist.p, ctx->d_range.p, blk, sbeg,
+  const int blocks = (int)std::min<long long>((n + wpb - 1) / wpb, 148LL * 16);
+  k_eri_jk_warp<LA, LB, LC, LD, SCHWARZ, T><<<blocks, 32 * wpb, smem, st>>>(ctx->d_qlist.p, ctx->d_range.p, blk, sbeg,
                                                                        send, make_pairs(ctx), make_shells(ctx),
                                                                        ctx->d_boys.p, dg, Q);
   return cudaGetLastError();
@@ -986,14 +989,10 @@ static void pair_prims(const cqg_ctx *ctx, int a, int b, double prim_thresh, std
 
 // primitive-count bucket of a shell pair: warps of the ERI kernels see kets of one bucket
 static inline int prim_bucket(int np) {
-  if (np <= 1) return 0;
-  if (np <= 2) return 1;
-  if (np <= 4) return 2;
-  if (np <= 8) return 3;
-  if (np <= 16) return 4;
-  if (np <= 32) return 5;
-  if (np <= 64) return 6;
-  return 7;
+  static const int upper[CQG_NBUCKET - 1] = {1, 2, 3, 4, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64};
+  for (int b = 0; b < CQG_NBUCKET - 1; ++b)
+    if (np <= upper[b]) return b;
+  return CQG_NBUCKET - 1;
 }
 
 // build primitive-pair data for the current pair ordering and upload all pair arrays
@@ -1041,19 +1040,10 @@ static cudaError_t launch_eri(cqg_ctx *ctx, int blk, long long n, cudaStream_t s
   }
 }
 
-#define CLASS_TABLE(T)                                                                                   \
-  {QC(0, 0, 0, 0, T),                                                                                    \
-   QC(1, 0, 0, 0, T), QC(1, 0, 1, 0, T),                                                                 \
-   QC(1, 1, 0, 0, T), QC(1, 1, 1, 0, T), QC(1, 1, 1, 1, T),                                              \
-   QC(2, 0, 0, 0, T), QC(2, 0, 1, 0, T), QC(2, 0, 1, 1, T), QC(2, 0, 2, 0, T),                           \
-   QC(2, 1, 0, 0, T), QC(2, 1, 1, 0, T), QC(2, 1, 1, 1, T), QC(2, 1, 2, 0, T), QC(2, 1, 2, 1, T),        \
-   QC(2, 2, 0, 0, T), QC(2, 2, 1, 0, T), QC(2, 2, 1, 1, T), QC(2, 2, 2, 0, T), QC(2, 2, 2, 1, T),        \
-   QC(2, 2, 2, 2, T)}
 #define QC(a, b, c, d, T) &launch_eri<a, b, c, d, T>
-static const eri_launcher kEriLaunch[CQG_NQC] = CLASS_TABLE(double);
-static const eri_launcher kEriLaunch32[CQG_NQC] = CLASS_TABLE(float);
+static const eri_launcher kEriLaunch[CQG_NQC] = CQG_CLASS_LIST(QC, double);
+static const eri_launcher kEriLaunch32[CQG_NQC] = CQG_CLASS_LIST(QC, float);
 #undef QC
-#undef CLASS_TABLE
 
 extern "C" {
 
@@ -1250,6 +1240,10 @@ cqg_status cqg_set_basis(cqg_ctx *ctx, int nshell, const int *L, const int *pure
   e = e ? e : launch_schwarz<2, 0>(ctx, P, S, ctx->pc_beg[3], ctx->pc_beg[4], dQ);
   e = e ? e : launch_schwarz<2, 1>(ctx, P, S, ctx->pc_beg[4], ctx->pc_beg[5], dQ);
   e = e ? e : launch_schwarz<2, 2>(ctx, P, S, ctx->pc_beg[5], ctx->pc_beg[6], dQ);
+  e = e ? e : launch_schwarz<3, 0>(ctx, P, S, ctx->pc_beg[6], ctx->pc_beg[7], dQ);
+  e = e ? e : launch_schwarz<3, 1>(ctx, P, S, ctx->pc_beg[7], ctx->pc_beg[8], dQ);
+  e = e ? e : launch_schwarz<3, 2>(ctx, P, S, ctx->pc_beg[8], ctx->pc_beg[9], dQ);
+  e = e ? e : launch_schwarz<3, 3>(ctx, P, S, ctx->pc_beg[9], ctx->pc_beg[10], dQ);
   if (e != cudaSuccess) {
     ctx->err = std::string("schwarz kernels: ") + cudaGetErrorString(e);
     return CQG_ERR_CUDA;

@@ -348,12 +348,14 @@ def quartet_classes(maxl):
 
 
 # classes evaluated by the warp-cooperative kernel (eri_warp.cuh): their Cartesian output
-# ncart(a)ncart(b)ncart(c)ncart(d) exceeds 150 values, too many for one thread's registers
+# ncart(a)ncart(b)ncart(c)ncart(d) exceeds 150 values or whose R_tuv set (L >= 6, 84+ values)
+# is too large for one thread's registers
 def _nc(l):
     return (l + 1) * (l + 2) // 2
 
 
-WARP_CLASSES = {q for q in quartet_classes(3) if _nc(q[0]) * _nc(q[1]) * _nc(q[2]) * _nc(q[3]) > 150}
+WARP_CLASSES = {q for q in quartet_classes(3)
+                if _nc(q[0]) * _nc(q[1]) * _nc(q[2]) * _nc(q[3]) > 150 or sum(q) >= 6}
 
 
 def main(path, maxl=2):
@@ -378,6 +380,12 @@ def main(path, maxl=2):
         parts.append("  }")
         parts.append("};")
         parts.append("")
+    qcs = quartet_classes(maxl)
+    parts.append("// quartet classes in engine order (bra pair class >= ket pair class)")
+    parts.append("#define CQG_CLASS_LIST(X, T) \\")
+    parts.append("  {" + ", ".join("X(%d, %d, %d, %d, T)" % q for q in qcs) + "}")
+    parts.append("#define CQG_GEN_MAXL %d" % maxl)
+    parts.append("")
     with open(path, "w") as f:
         f.write("\n".join(parts))
 

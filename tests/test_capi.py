@@ -46,7 +46,7 @@ def test_library_loads_and_answers_without_gpu():
     assert L.cqg_version().startswith(b"cqgpu")
     assert L.cqg_status_string(7) == b"unsupported input"
     names = _lib.class_names()
-    assert names[0] == "(ss|ss)" and names[-1] == "(dd|dd)" and len(names) == 21
+    assert names[0] == "(ss|ss)" and names[-1] == "(ff|ff)" and len(names) == 55
 
 
 def test_create_without_device_fails_cleanly():

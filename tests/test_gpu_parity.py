@@ -32,7 +32,7 @@ def oracle_G(ob, X, types, scale, thresh):
     return out, n
 
 
-@pytest.mark.parametrize("basis", ["sto-3g", "6-31g", "6-31g*", "cc-pvdz"])
+@pytest.mark.parametrize("basis", ["sto-3g", "6-31g", "6-31g*", "cc-pvdz", "cc-pvtz"])
 def test_water_rhf_G(basis):
     mol = single_water(1)
     bs = BasisSet(basis, mol.atoms, mol.coords)
@@ -72,8 +72,8 @@ def test_cluster_all_classes_formpt_uhf():
     assert st["quartets"] == nr
     assert np.abs(PTs - PTs_r).max() <= TOL_G
     assert np.abs(PTz - PTz_r).max() <= TOL_G
-    # every class up to (dd|dd) was exercised
-    assert all(v > 0 for v in st["class_quartets"].values() if v is not None)
+    # every class up to (dd|dd) was exercised (the first 21 of the 55 classes)
+    assert all(v > 0 for v in list(st["class_quartets"].values())[:21])
 
 
 def test_device_pointers_match_host():
@@ -155,3 +155,24 @@ def test_single_atom_and_diffuse_pair():
     Gr, nr = oracle_G(O.OracleBasis.from_basis(bs), [D, D], [0, 1], [1.0, -0.5], 1e-14)
     assert ints.stats()["quartets"] == nr
     assert np.abs(G - Gr).max() <= TOL_G
+
+
+def test_f_shell_classes_cc_pvtz_pair():
+    """Two waters in cc-pVTZ: every quartet class up to (ff|ff) (55 classes), UHF lists."""
+    mol = water_cluster(2, 17)
+    bs = BasisSet("cc-pvtz", mol.atoms, mol.coords)
+    ob = O.OracleBasis.from_basis(bs)
+    Ps = rand_sym(bs.nbasis, 31)
+    Pz = rand_sym(bs.nbasis, 32, 0.2)
+    ints = _aoi()(bs)
+    PTs, PTz = ints.formPT(Ps, Pz)
+    st = ints.stats()
+    PTs_r, PTz_r, nr = O.form_pt(ob, Ps, Pz)
+    assert st["quartets"] == nr
+    assert np.abs(PTs - PTs_r).max() <= TOL_G
+    assert np.abs(PTz - PTz_r).max() <= TOL_G
+    assert len(st["class_quartets"]) == 55 and st["class_quartets"]["(ff|ff)"] > 0
+    # Schwarz values of remote f pairs are square roots of tiny, cancellation-prone
+    # integrals: compare with a relative bar on the large ones and an absolute floor
+    Q = ints.computeSchwartz()
+    assert np.allclose(Q, O.schwarz(ob), rtol=1e-9, atol=1e-12)
