@@ -29,7 +29,7 @@ EXPORTED = [
     "cqg_version", "cqg_status_string", "cqg_create", "cqg_destroy", "cqg_last_error",
     "cqg_set_basis", "cqg_set_threshold", "cqg_set_precision", "cqg_get_schwarz",
     "cqg_get_sizes", "cqg_twoe_contract_direct", "cqg_form_pt", "cqg_get_stats",
-    "cqg_set_timing", "cqg_class_name", "cqg_probe_fma_peak", "cqg_one_e",
+    "cqg_set_timing", "cqg_class_name", "cqg_probe_fma_peak", "cqg_one_e", "cqg_set_list_budget",
 ]
 
 
@@ -44,6 +44,7 @@ class CqgStats(ctypes.Structure):
         ("ms_eri", ctypes.c_double),
         ("ms_total", ctypes.c_double),
         ("launches", ctypes.c_longlong),
+        ("chunks", ctypes.c_longlong),
         ("class_quartets", ctypes.c_longlong * 55),
         ("class_ms", ctypes.c_double * 55),
     ]
@@ -75,13 +76,15 @@ def load(path: str = LIB_PATH):
     L.cqg_form_pt.argtypes = [vp, ctypes.c_int, ctypes.c_double, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int, vp]
     L.cqg_get_stats.argtypes = [vp, ctypes.POINTER(CqgStats)]
     L.cqg_set_timing.argtypes = [vp, ctypes.c_int]
+    L.cqg_set_list_budget.argtypes = [vp, ctypes.c_longlong]
     L.cqg_class_name.argtypes = [ctypes.c_int]
     L.cqg_class_name.restype = ctypes.c_char_p
     L.cqg_probe_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, d]
     L.cqg_one_e.argtypes = [vp, ctypes.c_int, d, d, vp, vp, vp, ctypes.c_int, ctypes.c_int, vp]
     for name in ["cqg_create", "cqg_destroy", "cqg_set_basis", "cqg_set_threshold", "cqg_set_precision",
                  "cqg_get_schwarz", "cqg_get_sizes", "cqg_twoe_contract_direct", "cqg_form_pt",
-                 "cqg_get_stats", "cqg_set_timing", "cqg_probe_fma_peak", "cqg_one_e"]:
+                 "cqg_get_stats", "cqg_set_timing", "cqg_probe_fma_peak", "cqg_one_e",
+                 "cqg_set_list_budget"]:
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

@@ -111,6 +111,10 @@ class AOIntegrals:
     def setPrecision(self, policy: int, fp32_cutoff: float = 0.0):
         _lib.check(self._L.cqg_set_precision(self._ctx, int(policy), float(fp32_cutoff)), self._ctx)
 
+    def setListBudget(self, quartets: int):
+        """Largest number of quartets held in the device list at once (chunking above)."""
+        _lib.check(self._L.cqg_set_list_budget(self._ctx, int(quartets)), self._ctx)
+
     def setTiming(self, on: bool):
         _lib.check(self._L.cqg_set_timing(self._ctx, 1 if on else 0), self._ctx)
 
@@ -131,7 +135,7 @@ class AOIntegrals:
             "prim_quartets": int(s.prim_quartets), "model_flops": float(s.model_flops),
             "model_flops_fp32": float(s.model_flops_fp32),
             "ms_screen": s.ms_screen, "ms_eri": s.ms_eri, "ms_total": s.ms_total,
-            "launches": int(s.launches),
+            "launches": int(s.launches), "chunks": int(s.chunks),
             "class_quartets": {names[k]: int(s.class_quartets[k]) for k in range(len(names))},
             "class_ms": {names[k]: float(s.class_ms[k]) for k in range(len(names))},
         }

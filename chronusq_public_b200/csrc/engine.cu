@@ -216,17 +216,22 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
                                                   int nsh, const double *__restrict__ Mmax, double thresh,
                                                   double cut32, long long *__restrict__ cnt,
                                                   const long long *__restrict__ off, uint2 *__restrict__ qlist,
-                                                  unsigned long long *__restrict__ blkacc) {
+                                                  unsigned long long *__restrict__ blkacc, long long vt0,
+                                                  long long vt1, long long obase) {
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (warp >= ntask) return;
+  // fill pass: only the FP64 (virtual task warp) and FP32 (ntask + warp) parts inside the chunk
+  const bool do64 = !FILL || (warp >= vt0 && warp < vt1);
+  const bool do32 = !FILL || (ntask + warp >= vt0 && ntask + warp < vt1);
+  if (FILL && !do64 && !do32) return;
   int blk = find_block(bt, warp);
   int bra = bt.bra_beg[blk] + (warp - bt.task_beg[blk]);
   double qb = P.Q[bra];
   double mm = *Mmax;
   double cut = (qb * mm > 0.0) ? thresh / (qb * mm) * (1.0 - 1e-12) : 0.0;
   int2 ab = P.sh[bra];
-  const long long base64 = FILL ? off[warp] : 0, base32 = FILL ? off[ntask + warp] : 0;
+  const long long base64 = FILL ? off[warp] - obase : 0, base32 = FILL ? off[ntask + warp] - obase : 0;
   long long c64 = 0, c32 = 0;
   unsigned long long km64 = 0, ke64 = 0, km32 = 0, ke32 = 0;
   if (qb * mm > 0.0) {
@@ -246,8 +251,8 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
         const bool hi = pass && !lo;
         unsigned b64 = __ballot_sync(0xffffffffu, hi), b32 = __ballot_sync(0xffffffffu, lo);
         const unsigned below = (1u << lane) - 1u;
-        if (FILL && hi) qlist[base64 + c64 + __popc(b64 & below)] = make_uint2((unsigned)bra, (unsigned)ket);
-        if (FILL && lo) qlist[base32 + c32 + __popc(b32 & below)] = make_uint2((unsigned)bra, (unsigned)ket);
+        if (FILL && hi && do64) qlist[base64 + c64 + __popc(b64 & below)] = make_uint2((unsigned)bra, (unsigned)ket);
+        if (FILL && lo && do32) qlist[base32 + c32 + __popc(b32 & below)] = make_uint2((unsigned)bra, (unsigned)ket);
         if (!FILL && hi) {
           km64 += (unsigned long long)P.kk[ket];
           ke64 += (unsigned long long)P.np[ket];
@@ -839,6 +844,7 @@ struct cqg_ctx {
   int policy = CQG_PREC_FP64;
   double fp32_cutoff = 0.0;
   int timing = 0;
+  long long list_budget = 1LL << 29;   // quartets held in the list at once (8 B each)
   // basis
   int nshell = 0, nbf = 0, maxl = 0;
   std::vector<int> hL, hbf, hsz, hnprim, hpoff;
@@ -1136,6 +1142,12 @@ cqg_status cqg_set_precision(cqg_ctx *ctx, int policy, double cutoff) {
   return CQG_OK;
 }
 
+cqg_status cqg_set_list_budget(cqg_ctx *ctx, long long quartets) {
+  if (!ctx || quartets < 1) return CQG_ERR_BAD_ARG;
+  ctx->list_budget = quartets;
+  return CQG_OK;
+}
+
 cqg_status cqg_set_timing(cqg_ctx *ctx, int on) {
   if (!ctx) return CQG_ERR_BAD_ARG;
   ctx->timing = on ? 1 : 0;
@@ -1355,7 +1367,7 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     int nthr = 256, wpb = nthr / 32;
     int nb = (ctx->ntask + wpb - 1) / wpb;
     k_quartets<false><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, nsh, ctx->d_Mmax.p, ctx->thresh,
-                                            cut32, ctx->d_cnt.p, nullptr, nullptr, ctx->d_blkacc.p);
+                                            cut32, ctx->d_cnt.p, nullptr, nullptr, ctx->d_blkacc.p, 0, 0, 0);
     CUCHK(cudaGetLastError());
     size_t scan_bytes = ctx->d_scan_tmp.n;
     CUCHK(cub::DeviceScan::ExclusiveSum(ctx->d_scan_tmp.p, scan_bytes, ctx->d_cnt.p, ctx->d_off.p, 2 * ctx->ntask, st));
@@ -1379,20 +1391,43 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     return CQG_ERR_UNSUPPORTED;
   }
   long long total = hr[4 * CQG_NQC - 1];
-  if (ctx->d_qlist.reserve((size_t)std::max<long long>(total, 1)) != cudaSuccess) {
+  // The list is [FP64 part of every task][FP32 part of every task] ("virtual tasks"
+  // 0 .. 2 ntask).  It is filled and consumed in chunks of at most `list_budget` quartets.
+  const long long budget = std::max<long long>(ctx->list_budget, 1);
+  std::vector<long long> chunk_vt;   // chunk boundaries in virtual tasks
+  std::vector<long long> hoff, hcnt;
+  const long long nvt = 2LL * ctx->ntask;
+  if (total <= budget) {
+    chunk_vt = {0, nvt};
+  } else {
+    hoff.resize(nvt);
+    hcnt.resize(nvt);
+    CUCHK(cudaMemcpyAsync(hoff.data(), ctx->d_off.p, nvt * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CUCHK(cudaMemcpyAsync(hcnt.data(), ctx->d_cnt.p, nvt * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CUCHK(cudaStreamSynchronize(st));
+    chunk_vt.push_back(0);
+    long long start = 0;
+    for (long long v = 0; v < nvt; ++v) {
+      if (hoff[v] + hcnt[v] - start > budget && v > chunk_vt.back()) {
+        chunk_vt.push_back(v);
+        start = hoff[v];
+      }
+    }
+    chunk_vt.push_back(nvt);
+  }
+  long long cap = std::min(total, budget);
+  if (chunk_vt.size() > 2) {   // a single task may exceed the budget: size to the largest chunk
+    cap = 0;
+    for (size_t c = 0; c + 1 < chunk_vt.size(); ++c) {
+      const long long v0 = chunk_vt[c], v1 = chunk_vt[c + 1];
+      cap = std::max(cap, hoff[v1 - 1] + hcnt[v1 - 1] - hoff[v0]);
+    }
+  }
+  if (ctx->d_qlist.reserve((size_t)std::max<long long>(cap, 1)) != cudaSuccess) {
     ctx->err = "quartet list allocation failed";
     return CQG_ERR_OOM;
   }
-  {
-    int nthr = 256, wpb = nthr / 32;
-    int nb = (ctx->ntask + wpb - 1) / wpb;
-    k_quartets<true><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, nsh, ctx->d_Mmax.p, ctx->thresh,
-                                           cut32, nullptr, ctx->d_off.p, ctx->d_qlist.p, nullptr);
-    CUCHK(cudaGetLastError());
-    ctx->launches += 1;
-  }
-  if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[1], st));
-  // 3. ERI + digest per class
+  ctx->stats.chunks = (long long)chunk_vt.size() - 1;
   if (ctx->d_G.reserve((size_t)ngroups * n * n) != cudaSuccess) return CQG_ERR_OOM;
   CUCHK(cudaMemsetAsync(ctx->d_G.p, 0, (size_t)ngroups * n * n * sizeof(double), st));
   DigestGroups dg;
@@ -1422,16 +1457,56 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     mflops += (double)hacc[4 * k] * fp + (double)n64 * fd;
     mflops32 += (double)hacc[4 * k + 2] * fp + (double)n32 * fd;
     nprimq += (long long)(hacc[4 * k + 1] + hacc[4 * k + 3]);
-    if (n64 > 0) ctx->launches += 1;
-    if (n32 > 0) ctx->launches += 1;
-    if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[4 + 2 * k], st));
-    cudaError_t e = kEriLaunch[k](ctx, k, n64, st, dg);
-    if (e == cudaSuccess) e = kEriLaunch32[k](ctx, CQG_NQC + k, n32, st, dg);
-    if (e != cudaSuccess) {
-      ctx->err = std::string("eri kernel ") + cqg_class_name(k) + ": " + cudaGetErrorString(e);
-      return CQG_ERR_CUDA;
+  }
+  bool first_chunk = true;
+  for (size_t ch = 0; ch + 1 < chunk_vt.size(); ++ch) {
+    const long long vt0 = chunk_vt[ch], vt1 = chunk_vt[ch + 1];
+    long long obase = 0;
+    long long crange[4 * CQG_NQC];
+    if (chunk_vt.size() > 2) {
+      obase = hoff[vt0];
+      for (int vb = 0; vb < 2 * CQG_NQC; ++vb) {
+        const int prec = vb / CQG_NQC, b = vb % CQG_NQC;
+        long long t0 = (long long)prec * ctx->ntask + ctx->bt.task_beg[b];
+        long long t1 = (long long)prec * ctx->ntask + ctx->bt.task_beg[b + 1];
+        t0 = std::max(t0, vt0);
+        t1 = std::min(t1, vt1);
+        if (t1 > t0) {
+          crange[2 * vb] = hoff[t0] - obase;
+          crange[2 * vb + 1] = hoff[t1 - 1] + hcnt[t1 - 1] - obase;
+        } else {
+          crange[2 * vb] = crange[2 * vb + 1] = 0;
+        }
+      }
+      CUCHK(cudaMemcpyAsync(ctx->d_range.p, crange, sizeof(crange), cudaMemcpyHostToDevice, st));
+    } else {
+      for (int q = 0; q < 4 * CQG_NQC; ++q) crange[q] = hr[q];
     }
-    if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[5 + 2 * k], st));
+    {
+      int nthr = 256, wpb = nthr / 32;
+      int nb = (ctx->ntask + wpb - 1) / wpb;
+      k_quartets<true><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, nsh, ctx->d_Mmax.p, ctx->thresh,
+                                             cut32, nullptr, ctx->d_off.p, ctx->d_qlist.p, nullptr, vt0, vt1, obase);
+      CUCHK(cudaGetLastError());
+      ctx->launches += 1;
+    }
+    if (ctx->timing && first_chunk) CUCHK(cudaEventRecord(ctx->ev[1], st));
+    // 3. ERI + digest per class
+    for (int k = 0; k < CQG_NQC; ++k) {
+      const long long n64 = crange[2 * k + 1] - crange[2 * k];
+      const long long n32 = crange[2 * (CQG_NQC + k) + 1] - crange[2 * (CQG_NQC + k)];
+      if (n64 > 0) ctx->launches += 1;
+      if (n32 > 0) ctx->launches += 1;
+      if (ctx->timing && first_chunk) CUCHK(cudaEventRecord(ctx->ev[4 + 2 * k], st));
+      cudaError_t e = kEriLaunch[k](ctx, k, n64, st, dg);
+      if (e == cudaSuccess) e = kEriLaunch32[k](ctx, CQG_NQC + k, n32, st, dg);
+      if (e != cudaSuccess) {
+        ctx->err = std::string("eri kernel ") + cqg_class_name(k) + ": " + cudaGetErrorString(e);
+        return CQG_ERR_CUDA;
+      }
+      if (ctx->timing && first_chunk) CUCHK(cudaEventRecord(ctx->ev[5 + 2 * k], st));
+    }
+    first_chunk = false;
   }
   if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[2], st));
   // 4. AX += 0.5 (Gh + Gh^T)

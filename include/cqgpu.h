@@ -59,6 +59,7 @@ typedef struct {
   double ms_eri;                   /* device time of ERI + digest kernels (ms) */
   double ms_total;                 /* device time of the whole call (ms) */
   long long launches;              /* kernels of this library launched by the call */
+  long long chunks;                /* quartet-list chunks the call was processed in */
   long long class_quartets[55];    /* per quartet class (index: see cqg_class_name) */
   double class_ms[55];             /* device time per class kernel (ms), if timing on */
 } cqg_stats;
@@ -121,6 +122,9 @@ cqg_status cqg_one_e(cqg_ctx *ctx, int ncharge, const double *Z, const double *R
 
 /* Statistics of the last contraction (synchronises the context's stream). */
 cqg_status cqg_get_stats(cqg_ctx *ctx, cqg_stats *out);
+/* Largest number of quartets held in the device quartet list at once (8 bytes each;
+ * default 2^29).  Larger screened sets are filled and evaluated in chunks. */
+cqg_status cqg_set_list_budget(cqg_ctx *ctx, long long quartets);
 /* Per-class kernel timing on (1) / off (0, default). */
 cqg_status cqg_set_timing(cqg_ctx *ctx, int on);
 /* Name of quartet class index k ("(pp|ps)"), or NULL past the last class. */

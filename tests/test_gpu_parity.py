@@ -176,3 +176,19 @@ def test_f_shell_classes_cc_pvtz_pair():
     # integrals: compare with a relative bar on the large ones and an absolute floor
     Q = ints.computeSchwartz()
     assert np.allclose(Q, O.schwarz(ob), rtol=1e-9, atol=1e-12)
+
+
+def test_chunked_quartet_list_matches_single_pass():
+    """A quartet-list budget far below the screened count forces many fill/evaluate
+    chunks; the result must be identical to the one-pass build."""
+    mol = water_cluster(3, 7)
+    bs = BasisSet("cc-pvdz", mol.atoms, mol.coords)
+    D = rand_sym(bs.nbasis, 13)
+    ints = _aoi()(bs)
+    G1, _ = ints.formPT(D)
+    n1 = ints.stats()["quartets"]
+    ints.setListBudget(100000)
+    G2, _ = ints.formPT(D)
+    st = ints.stats()
+    assert st["chunks"] > 1 and st["quartets"] == n1
+    assert np.abs(G2 - G1).max() <= 1e-12
