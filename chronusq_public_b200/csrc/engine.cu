@@ -1497,14 +1497,22 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
       const long long n32 = crange[2 * (CQG_NQC + k) + 1] - crange[2 * (CQG_NQC + k)];
       if (n64 > 0) ctx->launches += 1;
       if (n32 > 0) ctx->launches += 1;
-      if (ctx->timing && first_chunk) CUCHK(cudaEventRecord(ctx->ev[4 + 2 * k], st));
+      if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[4 + 2 * k], st));
       cudaError_t e = kEriLaunch[k](ctx, k, n64, st, dg);
       if (e == cudaSuccess) e = kEriLaunch32[k](ctx, CQG_NQC + k, n32, st, dg);
       if (e != cudaSuccess) {
         ctx->err = std::string("eri kernel ") + cqg_class_name(k) + ": " + cudaGetErrorString(e);
         return CQG_ERR_CUDA;
       }
-      if (ctx->timing && first_chunk) CUCHK(cudaEventRecord(ctx->ev[5 + 2 * k], st));
+      if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[5 + 2 * k], st));
+    }
+    if (ctx->timing) {   // per-class device time, summed over chunks
+      CUCHK(cudaStreamSynchronize(st));
+      for (int k = 0; k < CQG_NQC; ++k) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ctx->ev[4 + 2 * k], ctx->ev[5 + 2 * k]) == cudaSuccess)
+          ctx->stats.class_ms[k] += ms;
+      }
     }
     first_chunk = false;
   }
@@ -1704,16 +1712,12 @@ cqg_status cqg_get_stats(cqg_ctx *ctx, cqg_stats *out) {
     float ms;
     cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
     s.ms_screen = ms;
-    cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
-    s.ms_eri = ms;
+    double eri = 0.0;
+    for (int k = 0; k < CQG_NQC; ++k) eri += s.class_ms[k];
+    s.ms_eri = eri;
     cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[3]);
     s.ms_total = ms;
-    for (int k = 0; k < CQG_NQC; ++k) {
-      if (s.class_quartets[k] > 0) {
-        cudaEventElapsedTime(&ms, ctx->ev[4 + 2 * k], ctx->ev[5 + 2 * k]);
-        s.class_ms[k] = ms;
-      }
-    }
+
   }
   *out = s;
   return CQG_OK;
