@@ -30,6 +30,7 @@ EXPORTED = [
     "cqg_set_basis", "cqg_set_threshold", "cqg_set_precision", "cqg_get_schwarz",
     "cqg_get_sizes", "cqg_twoe_contract_direct", "cqg_form_pt", "cqg_get_stats",
     "cqg_set_timing", "cqg_class_name", "cqg_probe_fma_peak", "cqg_one_e", "cqg_set_list_budget",
+    "cqg_set_basis_batch", "cqg_get_batch_layout", "cqg_twoe_contract_direct_batch", "cqg_one_e_batch",
 ]
 
 
@@ -77,6 +78,11 @@ def load(path: str = LIB_PATH):
     L.cqg_get_stats.argtypes = [vp, ctypes.POINTER(CqgStats)]
     L.cqg_set_timing.argtypes = [vp, ctypes.c_int]
     L.cqg_set_list_budget.argtypes = [vp, ctypes.c_longlong]
+    L.cqg_set_basis_batch.argtypes = [vp, ctypes.c_int, i, i, i, i, d, d, d]
+    L.cqg_get_batch_layout.argtypes = [vp, i, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
+    L.cqg_twoe_contract_direct_batch.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.POINTER(vp), i, d,
+                                                 ctypes.c_char_p, vp]
+    L.cqg_one_e_batch.argtypes = [vp, i, d, d, vp, vp, vp, vp]
     L.cqg_class_name.argtypes = [ctypes.c_int]
     L.cqg_class_name.restype = ctypes.c_char_p
     L.cqg_probe_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, d]
@@ -84,7 +90,8 @@ def load(path: str = LIB_PATH):
     for name in ["cqg_create", "cqg_destroy", "cqg_set_basis", "cqg_set_threshold", "cqg_set_precision",
                  "cqg_get_schwarz", "cqg_get_sizes", "cqg_twoe_contract_direct", "cqg_form_pt",
                  "cqg_get_stats", "cqg_set_timing", "cqg_probe_fma_peak", "cqg_one_e",
-                 "cqg_set_list_budget"]:
+                 "cqg_set_list_budget", "cqg_set_basis_batch", "cqg_get_batch_layout",
+                 "cqg_twoe_contract_direct_batch", "cqg_one_e_batch"]:
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

@@ -74,7 +74,22 @@ static double md_v1_digest_flops(int la, int lb, int lc, int ld) {
 // ------------------------------------------------------------------ device data ---
 struct Shells {
   const double3 *center;
-  const int *bf;
+  const int *bf;     // first basis function of the shell within its molecule
+  const int *mol;    // molecule of the shell
+};
+
+// Per-molecule layout: a context holds nmol >= 1 molecules (a batch).  Matrices of
+// molecule m are packed at offset xoff[m] with leading dimension nbf[m]; with a single
+// molecule the caller's matrices are used in place (xoff[0] = 0, leading dimension ldx).
+struct Mols {
+  int nmol;
+  const int *shoff;              // first (global) shell of molecule m
+  const int *nsh;                // shells of molecule m
+  const long long *Moff;         // offset of molecule m's nsh_m x nsh_m block-norm matrix
+  const long long *xoff;         // offset of molecule m's matrices in packed storage
+  const int *nbf;                // basis functions of molecule m
+  const unsigned char *active;   // molecule m takes part in the call
+  const int *molbk;              // [m][ket pair class][bucket + 1]: first pair of each bucket
 };
 struct Pairs {
   const int2 *sh;       // (shell a, shell b), internal orientation L_a >= L_b
@@ -90,9 +105,27 @@ struct DigestGroups {
   double sJ[CQG_MAXG];
   double sK[CQG_MAXG];
   int ng;
-  int ldx;
-  int n;
+  int ldx;                        // leading dimension of X when nmol == 1
+  int batch;                      // matrices are packed per molecule (Mols.xoff / nbf)
+  const long long *xoff;
+  const int *nbf;
 };
+
+// base pointers and leading dimensions of molecule m's X and Gh
+__device__ __forceinline__ void mol_view(const DigestGroups &dg, int g, int m, const double *&X, double *&G,
+                                         size_t &ldx, size_t &ldg) {
+  if (dg.batch) {
+    const long long o = dg.xoff[m];
+    X = dg.X[g] + o;
+    G = dg.G[g] + o;
+    ldx = ldg = (size_t)dg.nbf[m];
+  } else {
+    X = dg.X[g];
+    G = dg.G[g];
+    ldx = dg.ldx;
+    ldg = (size_t)dg.nbf[0];
+  }
+}
 
 // ------------------------------------------------------------------ kernels ---
 // Schwarz: Q(ab) = sqrt(max_ij |(ij|ij)|) for pairs [beg, end) of one class.
@@ -121,17 +154,27 @@ struct XList {
   const double *X[8];
   int n;
 };
-__global__ void k_blocknorm(XList xl, int ldx, int nsh, const int *__restrict__ bf,
+__global__ void k_blocknorm(XList xl, int ldx, Mols mols, const int *__restrict__ bf,
                             const int *__restrict__ sz, double *__restrict__ M,
                             int *__restrict__ flags, double sym_tol) {
+  const int mol = blockIdx.z;
+  const int nsh = mols.nsh[mol];
   int s1 = blockIdx.x * blockDim.x + threadIdx.x;
   int s2 = blockIdx.y;
-  if (s1 >= nsh) return;
-  int r0 = bf[s1], c0 = bf[s2], nr = sz[s1], nc = sz[s2];
+  if (s1 >= nsh || s2 >= nsh) return;
+  double *Mm = M + mols.Moff[mol];
+  if (!mols.active[mol]) {
+    Mm[(size_t)s1 + (size_t)s2 * nsh] = 0.0;
+    return;
+  }
+  const int g1 = mols.shoff[mol] + s1, g2 = mols.shoff[mol] + s2;
+  int r0 = bf[g1], c0 = bf[g2], nr = sz[g1], nc = sz[g2];
+  if (mols.nmol > 1) ldx = mols.nbf[mol];
+  const long long xo = mols.nmol > 1 ? mols.xoff[mol] : 0;
   double mx = 0.0;
   int bad = 0, asym = 0;
   for (int m = 0; m < xl.n; ++m) {
-    const double *X = xl.X[m];
+    const double *X = xl.X[m] + xo;
     for (int c = 0; c < nc; ++c)
       for (int r = 0; r < nr; ++r) {
         double v = X[(size_t)(r0 + r) + (size_t)(c0 + c) * ldx];
@@ -142,7 +185,7 @@ __global__ void k_blocknorm(XList xl, int ldx, int nsh, const int *__restrict__ 
         if (fabs(v - t) > sym_tol * fmax(1.0, av)) asym = 1;
       }
   }
-  M[(size_t)s1 + (size_t)s2 * nsh] = mx;
+  Mm[(size_t)s1 + (size_t)s2 * nsh] = mx;
   if (bad) atomicOr(flags + 0, 1);
   if (asym) atomicOr(flags + 1, 1);
 }
@@ -173,7 +216,7 @@ struct BlockTable {
   int ket_beg[CQG_NQC];        // first ket pair (global index) of the block
   int ket_n[CQG_NQC];          // number of ket pairs of the block's ket class
   int diag[CQG_NQC];           // bra class == ket class
-  int ket_bucket[CQG_NQC][CQG_NBUCKET + 1];  // global start of each primitive bucket of the ket class
+  int ket_class[CQG_NQC];      // pair class of the ket
 };
 
 __device__ __forceinline__ int find_block(const BlockTable &bt, int task) {
@@ -195,9 +238,9 @@ __device__ __forceinline__ int coarse_range(const double *__restrict__ Q, int kb
 
 // Density-weighted Schwarz bound of a quartet: max of the six shell-block norms of the
 // density times Q_ab Q_cd (contract.h:112-131).
-__device__ __forceinline__ double quartet_bound(const double *__restrict__ M, int nsh, int2 ab, int2 cd, double qab,
-                                                double qcd) {
-  const int s1 = ab.x, s2 = ab.y, s3 = cd.x, s4 = cd.y;
+__device__ __forceinline__ double quartet_bound(const double *__restrict__ M, int nsh, int shoff, int2 ab, int2 cd,
+                                                double qab, double qcd) {
+  const int s1 = ab.x - shoff, s2 = ab.y - shoff, s3 = cd.x - shoff, s4 = cd.y - shoff;
   double m = M[s1 + (size_t)s4 * nsh];
   m = fmax(m, M[s2 + (size_t)s4 * nsh]);
   m = fmax(m, M[s3 + (size_t)s4 * nsh]);
@@ -213,7 +256,8 @@ __device__ __forceinline__ double quartet_bound(const double *__restrict__ M, in
 // (counts cnt[ntask + task], offsets off[ntask + task]); the rest to the FP64 list.
 template <bool FILL>
 __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pairs P, const double *__restrict__ M,
-                                                  int nsh, const double *__restrict__ Mmax, double thresh,
+                                                  Mols mols, const int *__restrict__ shmol,
+                                                  const double *__restrict__ Mmax, double thresh,
                                                   double cut32, long long *__restrict__ cnt,
                                                   const long long *__restrict__ off, uint2 *__restrict__ qlist,
                                                   unsigned long long *__restrict__ blkacc, long long vt0,
@@ -231,12 +275,16 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
   double mm = *Mmax;
   double cut = (qb * mm > 0.0) ? thresh / (qb * mm) * (1.0 - 1e-12) : 0.0;
   int2 ab = P.sh[bra];
+  const int mol = shmol[ab.x];
+  const int nsh = mols.nsh[mol], shoff = mols.shoff[mol];
+  const double *Mm = M + mols.Moff[mol];
+  const int *bkt = mols.molbk + ((size_t)mol * CQG_NPC + bt.ket_class[blk]) * (CQG_NBUCKET + 1);
   const long long base64 = FILL ? off[warp] - obase : 0, base32 = FILL ? off[ntask + warp] - obase : 0;
   long long c64 = 0, c32 = 0;
   unsigned long long km64 = 0, ke64 = 0, km32 = 0, ke32 = 0;
-  if (qb * mm > 0.0) {
+  if (qb * mm > 0.0 && mols.active[mol]) {
     for (int bk = 0; bk < CQG_NBUCKET; ++bk) {
-      const int kb = bt.ket_bucket[blk][bk], ke = bt.ket_bucket[blk][bk + 1];
+      const int kb = bkt[bk], ke = bkt[bk + 1];
       if (ke <= kb) continue;
       int kend = kb + coarse_range(P.Q, kb, ke - kb, cut);
       if (bt.diag[blk]) kend = min(kend, bra + 1);   // unique pairs of pairs: ket <= bra
@@ -244,7 +292,7 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
         int ket = k0 + lane;
         bool pass = false, lo = false;
         if (ket < kend) {
-          const double bnd = quartet_bound(M, nsh, ab, P.sh[ket], qb, P.Q[ket]);
+          const double bnd = quartet_bound(Mm, nsh, shoff, ab, P.sh[ket], qb, P.Q[ket]);
           pass = bnd >= thresh;
           lo = pass && bnd < cut32;
         }
@@ -323,12 +371,14 @@ __device__ __forceinline__ double warp_sum(double x) {
 // warp before one atomic per element.
 template <int NA, int NB, int NC, int ND>
 __device__ __forceinline__ void digest(const double *v, double deg, int a0, int b0, int c0, int d0,
-                                       const DigestGroups &dg, bool valid, bool bra_uniform) {
-  const size_t ld = dg.ldx, n = dg.n;
+                                       const DigestGroups &dg, bool valid, bool bra_uniform, int mol) {
   const int lane = threadIdx.x & 31;
   for (int g = 0; g < dg.ng; ++g) {
-    const double *__restrict__ X = dg.X[g];
-    double *G = dg.G[g];
+    const double *Xv;
+    double *G;
+    size_t ld, n;
+    mol_view(dg, g, mol, Xv, G, ld, n);
+    const double *__restrict__ X = Xv;
     const double sJ = dg.sJ[g] * deg;
     const double sK = 0.5 * dg.sK[g] * deg;
     if (dg.sJ[g] != 0.0) {
@@ -484,7 +534,7 @@ __device__ __forceinline__ void eri_jk_one(const uint2 *__restrict__ ql, long lo
   const unsigned bra0 = __shfl_sync(0xffffffffu, e.x, 0);
   const bool uniform = __all_sync(0xffffffffu, e.x == bra0);
   const double deg = (ab.x == ab.y ? 1.0 : 2.0) * (cd.x == cd.y ? 1.0 : 2.0) * (e.x == e.y ? 1.0 : 2.0);
-  digest<NA, NB, NC, ND>(v, deg, S.bf[ab.x], S.bf[ab.y], S.bf[cd.x], S.bf[cd.y], dg, valid, uniform);
+  digest<NA, NB, NC, ND>(v, deg, S.bf[ab.x], S.bf[ab.y], S.bf[cd.x], S.bf[cd.y], dg, valid, uniform, S.mol[ab.x]);
 }
 
 // ------------------------------------------------------------- warp-mode classes ---
@@ -696,13 +746,16 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
     }
     const double deg = (ab.x == ab.y ? 1.0 : 2.0) * (cdp.x == cdp.y ? 1.0 : 2.0) * (e.x == e.y ? 1.0 : 2.0);
     const int a0 = S.bf[ab.x], b0 = S.bf[ab.y], c0 = S.bf[cdp.x], d0 = S.bf[cdp.y];
-    const size_t ld = dg.ldx, n = dg.n;
+    const int mol = S.mol[ab.x];
     // staged blocks: X(d,c) [NC*ND], X(b,a) [NA*NB], X(b,d), X(a,c), X(b,c), X(a,d)
     double *xdc = Xs, *xba = xdc + NC * ND, *xbd = xba + NA * NB, *xac = xbd + NB * ND;
     double *xbc = xac + NA * NC, *xad = xbc + NB * NC;
     for (int g = 0; g < dg.ng; ++g) {
-      const double *__restrict__ Xm = dg.X[g];
-      double *G = dg.G[g];
+      const double *Xv;
+      double *G;
+      size_t ld, n;
+      mol_view(dg, g, mol, Xv, G, ld, n);
+      const double *__restrict__ Xm = Xv;
       const double sJ = dg.sJ[g] * deg, sK = 0.5 * dg.sK[g] * deg;
       __syncwarp();
       for (int k = lane; k < NC * ND; k += 32) xdc[k] = __ldg(Xm + (d0 + k % ND) + (c0 + k / ND) * ld);
@@ -768,9 +821,19 @@ static size_t warp_smem_bytes() {
   return 4 * ((WARP_BYTES + 15) / 16 * 16);
 }
 
-// AX += 0.5 (Gh + Gh^T)
-__global__ void k_finalize(const double *__restrict__ Gh, int n, double *__restrict__ AX, int ldax) {
+// AX += 0.5 (Gh + Gh^T), molecule blockIdx.z of the context
+__global__ void k_finalize(const double *__restrict__ Gh0, Mols mols, double *__restrict__ AX0, int ldax) {
   __shared__ double tile[32][33];
+  const int mol = blockIdx.z;
+  const int n = mols.nbf[mol];
+  if (!mols.active[mol] || (int)(blockIdx.x * 32) >= n || (int)(blockIdx.y * 32) >= n) return;
+  const double *Gh = Gh0;
+  double *AX = AX0;
+  if (mols.nmol > 1) {
+    Gh += mols.xoff[mol];
+    AX += mols.xoff[mol];
+    ldax = n;
+  }
   int bx = blockIdx.x * 32, by = blockIdx.y * 32;
   int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
   for (int k = ty; k < 32; k += 8) {
@@ -845,6 +908,15 @@ struct cqg_ctx {
   double fp32_cutoff = 0.0;
   int timing = 0;
   long long list_budget = 1LL << 29;   // quartets held in the list at once (8 B each)
+  // molecules of the context (a batch when nmol > 1)
+  int nmol = 0, max_nsh = 0, max_nbf = 0;
+  long long packed = 0, Mtotal = 0, nallpairs = 0;
+  std::vector<int> hshmol, m_shoff, m_nsh, m_nbf;
+  std::vector<long long> m_xoff, m_Moff;
+  std::vector<unsigned char> h_active;
+  DevBuf<int> d_shmol, d_mshoff, d_mnsh, d_mnbf, d_molbk;
+  DevBuf<long long> d_mxoff, d_mMoff;
+  DevBuf<unsigned char> d_active;
   // basis
   int nshell = 0, nbf = 0, maxl = 0;
   std::vector<int> hL, hbf, hsz, hnprim, hpoff;
@@ -959,7 +1031,20 @@ static Shells make_shells(cqg_ctx *ctx) {
   Shells S;
   S.center = ctx->d_center.p;
   S.bf = ctx->d_bf.p;
+  S.mol = ctx->d_shmol.p;
   return S;
+}
+static Mols make_mols(cqg_ctx *ctx) {
+  Mols M;
+  M.nmol = ctx->nmol;
+  M.shoff = ctx->d_mshoff.p;
+  M.nsh = ctx->d_mnsh.p;
+  M.Moff = ctx->d_mMoff.p;
+  M.xoff = ctx->d_mxoff.p;
+  M.nbf = ctx->d_mnbf.p;
+  M.active = ctx->d_active.p;
+  M.molbk = ctx->d_molbk.p;
+  return M;
 }
 
 // Primitive pairs of shell pair (a, b); prim_thresh = 0 keeps all of them, otherwise a
@@ -1117,6 +1202,8 @@ cqg_status cqg_destroy(cqg_ctx *ctx) {
   ctx->d_pair_kk.release(); ctx->d_blkacc.release();
   ctx->d_shL.release(); ctx->d_shnp.release(); ctx->d_shpoff.release(); ctx->d_alpha.release();
   ctx->d_coef.release(); ctx->d_allpairs.release(); ctx->d_oe.release(); ctx->d_charges.release();
+  ctx->d_shmol.release(); ctx->d_mshoff.release(); ctx->d_mnsh.release(); ctx->d_mnbf.release();
+  ctx->d_molbk.release(); ctx->d_mxoff.release(); ctx->d_mMoff.release(); ctx->d_active.release();
   ctx->d_prim.release(); ctx->d_boys.release();
   ctx->d_M.release(); ctx->d_Mmax.release(); ctx->d_flags.release();
   ctx->d_cnt.release(); ctx->d_off.release(); ctx->d_range.release(); ctx->d_scan_tmp.release();
@@ -1162,10 +1249,19 @@ cqg_status cqg_get_sizes(cqg_ctx *ctx, int *nshell, int *nbasis, int *maxl) {
   return CQG_OK;
 }
 
-cqg_status cqg_set_basis(cqg_ctx *ctx, int nshell, const int *L, const int *pure, const int *nprim,
-                         const double *alpha, const double *coef, const double *centers) {
-  if (!ctx || nshell <= 0 || !L || !pure || !nprim || !alpha || !coef || !centers) return CQG_ERR_BAD_ARG;
+cqg_status cqg_set_basis_batch(cqg_ctx *ctx, int nmol, const int *nshell_per_mol, const int *L, const int *pure,
+                               const int *nprim, const double *alpha, const double *coef, const double *centers) {
+  if (!ctx || nmol <= 0 || !nshell_per_mol || !L || !pure || !nprim || !alpha || !coef || !centers)
+    return CQG_ERR_BAD_ARG;
   CUCHK(cudaSetDevice(ctx->device));
+  int nshell = 0;
+  for (int m = 0; m < nmol; ++m) {
+    if (nshell_per_mol[m] <= 0) {
+      ctx->err = "molecule without shells";
+      return CQG_ERR_BAD_ARG;
+    }
+    nshell += nshell_per_mol[m];
+  }
   int tot = 0, maxl = 0;
   for (int s = 0; s < nshell; ++s) {
     if (L[s] < 0 || nprim[s] <= 0) {
@@ -1183,6 +1279,7 @@ cqg_status cqg_set_basis(cqg_ctx *ctx, int nshell, const int *L, const int *pure
     tot += nprim[s];
     maxl = std::max(maxl, L[s]);
   }
+  ctx->nmol = nmol;
   ctx->nshell = nshell;
   ctx->maxl = maxl;
   ctx->hL.assign(L, L + nshell);
@@ -1193,27 +1290,67 @@ cqg_status cqg_set_basis(cqg_ctx *ctx, int nshell, const int *L, const int *pure
   ctx->hbf.resize(nshell);
   ctx->hsz.resize(nshell);
   ctx->hpoff.resize(nshell);
-  int f = 0, p = 0;
-  for (int s = 0; s < nshell; ++s) {
-    ctx->hbf[s] = f;
-    ctx->hsz[s] = nfun(L[s]);
-    f += ctx->hsz[s];
-    ctx->hpoff[s] = p;
-    p += nprim[s];
+  ctx->hshmol.resize(nshell);
+  ctx->m_shoff.resize(nmol);
+  ctx->m_nsh.resize(nmol);
+  ctx->m_nbf.resize(nmol);
+  ctx->m_xoff.resize(nmol);
+  ctx->m_Moff.resize(nmol);
+  {
+    int p = 0, s = 0;
+    long long xo = 0, mo = 0;
+    ctx->max_nsh = 0;
+    ctx->max_nbf = 0;
+    for (int m = 0; m < nmol; ++m) {
+      ctx->m_shoff[m] = s;
+      ctx->m_nsh[m] = nshell_per_mol[m];
+      int f = 0;
+      for (int k = 0; k < nshell_per_mol[m]; ++k, ++s) {
+        ctx->hbf[s] = f;
+        ctx->hsz[s] = nfun(L[s]);
+        f += ctx->hsz[s];
+        ctx->hpoff[s] = p;
+        p += nprim[s];
+        ctx->hshmol[s] = m;
+      }
+      ctx->m_nbf[m] = f;
+      ctx->m_xoff[m] = xo;
+      ctx->m_Moff[m] = mo;
+      xo += (long long)f * f;
+      mo += (long long)nshell_per_mol[m] * nshell_per_mol[m];
+      ctx->max_nsh = std::max(ctx->max_nsh, nshell_per_mol[m]);
+      ctx->max_nbf = std::max(ctx->max_nbf, f);
+    }
+    ctx->packed = xo;
+    ctx->Mtotal = mo;
   }
-  ctx->nbf = f;
-  // shells to device
+  ctx->nbf = ctx->m_nbf[0];
+  // shells and molecule layout to device
   std::vector<double3> c3(nshell);
   for (int s = 0; s < nshell; ++s) c3[s] = make_double3(centers[3 * s], centers[3 * s + 1], centers[3 * s + 2]);
-  if (ctx->d_center.reserve(nshell) || ctx->d_bf.reserve(nshell) || ctx->d_sz.reserve(nshell)) return CQG_ERR_OOM;
+  if (ctx->d_center.reserve(nshell) || ctx->d_bf.reserve(nshell) || ctx->d_sz.reserve(nshell) ||
+      ctx->d_shmol.reserve(nshell) || ctx->d_mshoff.reserve(nmol) || ctx->d_mnsh.reserve(nmol) ||
+      ctx->d_mnbf.reserve(nmol) || ctx->d_mxoff.reserve(nmol) || ctx->d_mMoff.reserve(nmol) ||
+      ctx->d_active.reserve(nmol))
+    return CQG_ERR_OOM;
   CUCHK(cudaMemcpy(ctx->d_center.p, c3.data(), nshell * sizeof(double3), cudaMemcpyHostToDevice));
   CUCHK(cudaMemcpy(ctx->d_bf.p, ctx->hbf.data(), nshell * sizeof(int), cudaMemcpyHostToDevice));
   CUCHK(cudaMemcpy(ctx->d_sz.p, ctx->hsz.data(), nshell * sizeof(int), cudaMemcpyHostToDevice));
-  // raw shells (one-electron integrals) and the list of all pairs a >= b
+  CUCHK(cudaMemcpy(ctx->d_shmol.p, ctx->hshmol.data(), nshell * sizeof(int), cudaMemcpyHostToDevice));
+  CUCHK(cudaMemcpy(ctx->d_mshoff.p, ctx->m_shoff.data(), nmol * sizeof(int), cudaMemcpyHostToDevice));
+  CUCHK(cudaMemcpy(ctx->d_mnsh.p, ctx->m_nsh.data(), nmol * sizeof(int), cudaMemcpyHostToDevice));
+  CUCHK(cudaMemcpy(ctx->d_mnbf.p, ctx->m_nbf.data(), nmol * sizeof(int), cudaMemcpyHostToDevice));
+  CUCHK(cudaMemcpy(ctx->d_mxoff.p, ctx->m_xoff.data(), nmol * sizeof(long long), cudaMemcpyHostToDevice));
+  CUCHK(cudaMemcpy(ctx->d_mMoff.p, ctx->m_Moff.data(), nmol * sizeof(long long), cudaMemcpyHostToDevice));
+  ctx->h_active.assign(nmol, 1);
+  CUCHK(cudaMemcpy(ctx->d_active.p, ctx->h_active.data(), nmol, cudaMemcpyHostToDevice));
+  // raw shells (one-electron integrals) and the list of all pairs a >= b within each molecule
   {
     std::vector<int2> allp;
-    for (int a = 0; a < nshell; ++a)
-      for (int b = 0; b <= a; ++b) allp.push_back(make_int2(a, b));
+    for (int m = 0; m < nmol; ++m)
+      for (int a = ctx->m_shoff[m]; a < ctx->m_shoff[m] + ctx->m_nsh[m]; ++a)
+        for (int b = ctx->m_shoff[m]; b <= a; ++b) allp.push_back(make_int2(a, b));
+    ctx->nallpairs = (long long)allp.size();
     if (ctx->d_shL.reserve(nshell) || ctx->d_shnp.reserve(nshell) || ctx->d_shpoff.reserve(nshell) ||
         ctx->d_alpha.reserve(tot) || ctx->d_coef.reserve(tot) || ctx->d_allpairs.reserve(allp.size()))
       return CQG_ERR_OOM;
@@ -1224,14 +1361,15 @@ cqg_status cqg_set_basis(cqg_ctx *ctx, int nshell, const int *L, const int *pure
     CUCHK(cudaMemcpy(ctx->d_coef.p, coef, tot * sizeof(double), cudaMemcpyHostToDevice));
     CUCHK(cudaMemcpy(ctx->d_allpairs.p, allp.data(), allp.size() * sizeof(int2), cudaMemcpyHostToDevice));
   }
-  // pairs by class, internal orientation L_a >= L_b (a >= b when equal L)
+  // pairs within each molecule, by class, internal orientation L_a >= L_b (a >= b when equal L)
   std::vector<std::vector<int2>> bycls(CQG_NPC);
-  for (int a = 0; a < nshell; ++a)
-    for (int b = 0; b <= a; ++b) {
-      int x = a, y = b;
-      if (L[y] > L[x]) std::swap(x, y);
-      bycls[pair_class_of(L[x], L[y])].push_back(make_int2(x, y));
-    }
+  for (int m = 0; m < nmol; ++m)
+    for (int a = ctx->m_shoff[m]; a < ctx->m_shoff[m] + ctx->m_nsh[m]; ++a)
+      for (int b = ctx->m_shoff[m]; b <= a; ++b) {
+        int x = a, y = b;
+        if (L[y] > L[x]) std::swap(x, y);
+        bycls[pair_class_of(L[x], L[y])].push_back(make_int2(x, y));
+      }
   ctx->pair_sh.clear();
   for (int c = 0; c < CQG_NPC; ++c) {
     ctx->pc_beg[c] = (int)ctx->pair_sh.size();
@@ -1262,14 +1400,18 @@ cqg_status cqg_set_basis(cqg_ctx *ctx, int nshell, const int *L, const int *pure
   }
   CUCHK(cudaDeviceSynchronize());
   CUCHK(cudaMemcpy(ctx->pair_Q.data(), dQ, ctx->pair_Q.size() * sizeof(double), cudaMemcpyDeviceToHost));
-  ctx->Qmat.assign((size_t)nshell * nshell, 0.0);
-  for (size_t i = 0; i < ctx->pair_sh.size(); ++i) {
-    int a = ctx->pair_sh[i].x, b = ctx->pair_sh[i].y;
-    ctx->Qmat[a + (size_t)b * nshell] = ctx->pair_Q[i];
-    ctx->Qmat[b + (size_t)a * nshell] = ctx->pair_Q[i];
+  if (nmol == 1) {
+    ctx->Qmat.assign((size_t)nshell * nshell, 0.0);
+    for (size_t i = 0; i < ctx->pair_sh.size(); ++i) {
+      int a = ctx->pair_sh[i].x, b = ctx->pair_sh[i].y;
+      ctx->Qmat[a + (size_t)b * nshell] = ctx->pair_Q[i];
+      ctx->Qmat[b + (size_t)a * nshell] = ctx->pair_Q[i];
+    }
+  } else {
+    ctx->Qmat.clear();
   }
-  // sort each class by (primitive-count bucket, Q descending), stable, and rebuild with
-  // primitive-pair screening; bucket starts go to the block table
+  // sort each class by (molecule, primitive-count bucket, Q descending), stable, and
+  // rebuild with primitive-pair screening; per (molecule, class) bucket starts -> molbk
   std::vector<int> npscr(ctx->pair_sh.size());
   {
     std::vector<PrimPair> tmp;
@@ -1279,19 +1421,36 @@ cqg_status cqg_set_basis(cqg_ctx *ctx, int nshell, const int *L, const int *pure
       npscr[i] = (int)tmp.size();
     }
   }
+  const int NB1 = CQG_NBUCKET + 1;
+  std::vector<int> molbk((size_t)nmol * CQG_NPC * NB1, 0);
   for (int c = 0; c < CQG_NPC; ++c) {
     int b0 = ctx->pc_beg[c], b1 = ctx->pc_beg[c + 1];
     std::vector<int> idx(b1 - b0);
     std::iota(idx.begin(), idx.end(), b0);
     std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
+      int mx = ctx->hshmol[ctx->pair_sh[x].x], my = ctx->hshmol[ctx->pair_sh[y].x];
+      if (mx != my) return mx < my;
       int bx = prim_bucket(npscr[x]), by = prim_bucket(npscr[y]);
       if (bx != by) return bx < by;
       return ctx->pair_Q[x] > ctx->pair_Q[y];
     });
-    for (int bk = 0; bk <= CQG_NBUCKET; ++bk) ctx->bucket_beg[c][bk] = b1;
-    for (int k = (int)idx.size() - 1; k >= 0; --k) ctx->bucket_beg[c][prim_bucket(npscr[idx[k]])] = b0 + k;
-    for (int bk = CQG_NBUCKET - 1; bk >= 0; --bk)
-      if (ctx->bucket_beg[c][bk] > ctx->bucket_beg[c][bk + 1]) ctx->bucket_beg[c][bk] = ctx->bucket_beg[c][bk + 1];
+    // bucket starts per molecule: first index of (m, bk); empty buckets start where the next begins
+    std::vector<int> first((size_t)nmol * NB1, -1);
+    for (int k = 0; k < (int)idx.size(); ++k) {
+      const int m = ctx->hshmol[ctx->pair_sh[idx[k]].x], bk = prim_bucket(npscr[idx[k]]);
+      if (first[(size_t)m * NB1 + bk] < 0) first[(size_t)m * NB1 + bk] = b0 + k;
+    }
+    int next = b1;
+    for (int m = nmol - 1; m >= 0; --m) {
+      int *row = &molbk[((size_t)m * CQG_NPC + c) * NB1];
+      row[CQG_NBUCKET] = next;
+      for (int bk = CQG_NBUCKET - 1; bk >= 0; --bk) {
+        const int f = first[(size_t)m * NB1 + bk];
+        row[bk] = f >= 0 ? f : row[bk + 1];
+      }
+      next = row[0];
+    }
+    for (int bk = 0; bk <= CQG_NBUCKET; ++bk) ctx->bucket_beg[c][bk] = molbk[(size_t)c * NB1 + bk];
     std::vector<int2> sh2;
     std::vector<double> q2;
     for (int i : idx) {
@@ -1301,6 +1460,8 @@ cqg_status cqg_set_basis(cqg_ctx *ctx, int nshell, const int *L, const int *pure
     std::copy(sh2.begin(), sh2.end(), ctx->pair_sh.begin() + b0);
     std::copy(q2.begin(), q2.end(), ctx->pair_Q.begin() + b0);
   }
+  if (ctx->d_molbk.reserve(molbk.size())) return CQG_ERR_OOM;
+  CUCHK(cudaMemcpy(ctx->d_molbk.p, molbk.data(), molbk.size() * sizeof(int), cudaMemcpyHostToDevice));
   st = upload_pairs(ctx, 1e-24);
   if (st != CQG_OK) return st;
   // class-block table
@@ -1314,7 +1475,7 @@ cqg_status cqg_set_basis(cqg_ctx *ctx, int nshell, const int *L, const int *pure
     bt.bra_beg[k] = ctx->pc_beg[i];
     bt.ket_beg[k] = ctx->pc_beg[j];
     bt.ket_n[k] = ctx->pc_beg[j + 1] - ctx->pc_beg[j];
-    for (int bk = 0; bk <= CQG_NBUCKET; ++bk) bt.ket_bucket[k][bk] = ctx->bucket_beg[j][bk];
+    bt.ket_class[k] = j;
     bt.diag[k] = (i == j);
     task += ctx->pc_beg[i + 1] - ctx->pc_beg[i];
   }
@@ -1324,10 +1485,15 @@ cqg_status cqg_set_basis(cqg_ctx *ctx, int nshell, const int *L, const int *pure
   size_t scan_bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (long long *)nullptr, (long long *)nullptr, std::max(2 * task, 1));
   if (ctx->d_cnt.reserve(2 * task + 1) || ctx->d_off.reserve(2 * task + 1) || ctx->d_range.reserve(4 * CQG_NQC) ||
-      ctx->d_scan_tmp.reserve(scan_bytes + 16) || ctx->d_M.reserve((size_t)nshell * nshell) ||
+      ctx->d_scan_tmp.reserve(scan_bytes + 16) || ctx->d_M.reserve((size_t)std::max(ctx->Mtotal, 1LL)) ||
       ctx->d_Mmax.reserve(1) || ctx->d_flags.reserve(4) || ctx->d_blkacc.reserve(4 * CQG_NQC))
     return CQG_ERR_OOM;
   return CQG_OK;
+}
+
+cqg_status cqg_set_basis(cqg_ctx *ctx, int nshell, const int *L, const int *pure, const int *nprim,
+                         const double *alpha, const double *coef, const double *centers) {
+  return cqg_set_basis_batch(ctx, 1, &nshell, L, pure, nprim, alpha, coef, centers);
 }
 
 cqg_status cqg_get_schwarz(cqg_ctx *ctx, double *Q) {
@@ -1340,7 +1506,10 @@ cqg_status cqg_get_schwarz(cqg_ctx *ctx, double *Q) {
 static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const *Xg, double *const *AXg,
                                   const double *sJ, const double *sK, int nx_all, const double *const *Xall,
                                   int ldx, int ldax, cudaStream_t st) {
-  const int n = ctx->nbf, nsh = ctx->nshell;
+  const int n = ctx->nbf;
+  const Mols mols = make_mols(ctx);
+  // Gh of every molecule: n x n for one molecule, packed per molecule for a batch
+  const size_t gsize = ctx->nmol > 1 ? (size_t)ctx->packed : (size_t)n * n;
   if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[0], st));
   // 1. block norms + checks
   XList xl;
@@ -1352,10 +1521,10 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
   const double cut32 = ctx->policy == CQG_PREC_MIXED ? ctx->fp32_cutoff : 0.0;
   ctx->launches = 0;
   {
-    dim3 g((nsh + 127) / 128, nsh);
-    k_blocknorm<<<g, 128, 0, st>>>(xl, ldx, nsh, ctx->d_bf.p, ctx->d_sz.p, ctx->d_M.p, ctx->d_flags.p, 1e-12);
+    dim3 g((ctx->max_nsh + 127) / 128, ctx->max_nsh, ctx->nmol);
+    k_blocknorm<<<g, 128, 0, st>>>(xl, ldx, mols, ctx->d_bf.p, ctx->d_sz.p, ctx->d_M.p, ctx->d_flags.p, 1e-12);
     CUCHK(cudaGetLastError());
-    long long nn = (long long)nsh * nsh;
+    long long nn = ctx->Mtotal;
     int nb = (int)std::min<long long>((nn + 255) / 256, 1184);
     k_maxreduce<<<nb, 256, 0, st>>>(ctx->d_M.p, nn, ctx->d_Mmax.p);
     CUCHK(cudaGetLastError());
@@ -1366,7 +1535,8 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
   {
     int nthr = 256, wpb = nthr / 32;
     int nb = (ctx->ntask + wpb - 1) / wpb;
-    k_quartets<false><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, nsh, ctx->d_Mmax.p, ctx->thresh,
+    k_quartets<false><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
+                                            ctx->thresh,
                                             cut32, ctx->d_cnt.p, nullptr, nullptr, ctx->d_blkacc.p, 0, 0, 0);
     CUCHK(cudaGetLastError());
     size_t scan_bytes = ctx->d_scan_tmp.n;
@@ -1428,16 +1598,18 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     return CQG_ERR_OOM;
   }
   ctx->stats.chunks = (long long)chunk_vt.size() - 1;
-  if (ctx->d_G.reserve((size_t)ngroups * n * n) != cudaSuccess) return CQG_ERR_OOM;
-  CUCHK(cudaMemsetAsync(ctx->d_G.p, 0, (size_t)ngroups * n * n * sizeof(double), st));
+  if (ctx->d_G.reserve((size_t)ngroups * gsize) != cudaSuccess) return CQG_ERR_OOM;
+  CUCHK(cudaMemsetAsync(ctx->d_G.p, 0, (size_t)ngroups * gsize * sizeof(double), st));
   DigestGroups dg;
   memset(&dg, 0, sizeof(dg));
   dg.ng = ngroups;
   dg.ldx = ldx;
-  dg.n = n;
+  dg.batch = ctx->nmol > 1;
+  dg.xoff = ctx->d_mxoff.p;
+  dg.nbf = ctx->d_mnbf.p;
   for (int g = 0; g < ngroups; ++g) {
     dg.X[g] = Xg[g];
-    dg.G[g] = ctx->d_G.p + (size_t)g * n * n;
+    dg.G[g] = ctx->d_G.p + (size_t)g * gsize;
     dg.sJ[g] = sJ[g];
     dg.sK[g] = sK[g];
   }
@@ -1485,7 +1657,8 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     {
       int nthr = 256, wpb = nthr / 32;
       int nb = (ctx->ntask + wpb - 1) / wpb;
-      k_quartets<true><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, nsh, ctx->d_Mmax.p, ctx->thresh,
+      k_quartets<true><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
+                                             ctx->thresh,
                                              cut32, nullptr, ctx->d_off.p, ctx->d_qlist.p, nullptr, vt0, vt1, obase);
       CUCHK(cudaGetLastError());
       ctx->launches += 1;
@@ -1519,8 +1692,8 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
   if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[2], st));
   // 4. AX += 0.5 (Gh + Gh^T)
   for (int g = 0; g < ngroups; ++g) {
-    dim3 grid((n + 31) / 32, (n + 31) / 32), blk(32, 8);
-    k_finalize<<<grid, blk, 0, st>>>(dg.G[g], n, AXg[g], ldax);
+    dim3 grid((ctx->max_nbf + 31) / 32, (ctx->max_nbf + 31) / 32, ctx->nmol), blk(32, 8);
+    k_finalize<<<grid, blk, 0, st>>>(dg.G[g], mols, AXg[g], ldax);
     CUCHK(cudaGetLastError());
     ctx->launches += 1;
   }
@@ -1687,10 +1860,16 @@ cqg_status cqg_one_e(cqg_ctx *ctx, int ncharge, const double *Z, const double *R
   sh.alpha = ctx->d_alpha.p;
   sh.coef = ctx->d_coef.p;
   sh.center = ctx->d_center.p;
-  const int np = ctx->nshell * (ctx->nshell + 1) / 2;
-  k_one_e<<<(np + 63) / 64, 64, 0, st>>>(sh, ctx->d_allpairs.p, np, ncharge, ctx->d_charges.p,
-                                         (const double3 *)(ctx->d_charges.p + ncharge), ctx->d_boys.p, dS, dT, dV,
-                                         ldd);
+  if (ctx->nmol != 1) {
+    ctx->err = "cqg_one_e is for single-molecule contexts; use cqg_one_e_batch";
+    return CQG_ERR_STATE;
+  }
+  const long long np = ctx->nallpairs;
+  OneEMols om;
+  memset(&om, 0, sizeof(om));
+  k_one_e<<<(unsigned)((np + 63) / 64), 64, 0, st>>>(sh, ctx->d_allpairs.p, np, ncharge, ctx->d_charges.p,
+                                                     (const double3 *)(ctx->d_charges.p + ncharge), ctx->d_boys.p, dS,
+                                                     dT, dV, ldd, om);
   CUCHK(cudaGetLastError());
   if (!on_device) {
     double *outs[3] = {S, T, V};
@@ -1701,6 +1880,92 @@ cqg_status cqg_one_e(cqg_ctx *ctx, int ncharge, const double *Z, const double *R
     CUCHK(cudaStreamSynchronize(st));
   }
   return CQG_OK;
+}
+
+cqg_status cqg_one_e_batch(cqg_ctx *ctx, const int *ncharge_per_mol, const double *Z, const double *R, double *S,
+                           double *T, double *V, void *stream) {
+  if (!ctx || !ncharge_per_mol || !Z || !R || !S || !T || !V) return CQG_ERR_BAD_ARG;
+  if (ctx->nshell == 0) return CQG_ERR_STATE;
+  CUCHK(cudaSetDevice(ctx->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nmol = ctx->nmol;
+  std::vector<int> coff(nmol + 1, 0);
+  for (int m = 0; m < nmol; ++m) coff[m + 1] = coff[m] + ncharge_per_mol[m];
+  const int nc = coff[nmol];
+  if (ctx->d_charges.reserve(4 * (size_t)std::max(nc, 1) + nmol + 1)) return CQG_ERR_OOM;
+  std::vector<double> zr(4 * (size_t)std::max(nc, 1) + nmol + 1, 0.0);
+  for (int c = 0; c < nc; ++c) {
+    zr[c] = Z[c];
+    zr[nc + 3 * c] = R[3 * c];
+    zr[nc + 3 * c + 1] = R[3 * c + 1];
+    zr[nc + 3 * c + 2] = R[3 * c + 2];
+  }
+  int *dcoff = (int *)(ctx->d_charges.p + 4 * (size_t)std::max(nc, 1));
+  CUCHK(cudaMemcpyAsync(ctx->d_charges.p, zr.data(), 4 * (size_t)std::max(nc, 1) * sizeof(double),
+                        cudaMemcpyHostToDevice, st));
+  CUCHK(cudaMemcpyAsync(dcoff, coff.data(), (nmol + 1) * sizeof(int), cudaMemcpyHostToDevice, st));
+  OneEShells sh;
+  sh.L = ctx->d_shL.p;
+  sh.nprim = ctx->d_shnp.p;
+  sh.poff = ctx->d_shpoff.p;
+  sh.bf = ctx->d_bf.p;
+  sh.alpha = ctx->d_alpha.p;
+  sh.coef = ctx->d_coef.p;
+  sh.center = ctx->d_center.p;
+  OneEMols om;
+  om.shmol = ctx->d_shmol.p;
+  om.xoff = ctx->d_mxoff.p;
+  om.nbf = ctx->d_mnbf.p;
+  om.coff = dcoff;
+  om.batch = 1;
+  const long long np = ctx->nallpairs;
+  k_one_e<<<(unsigned)((np + 63) / 64), 64, 0, st>>>(sh, ctx->d_allpairs.p, np, nc, ctx->d_charges.p,
+                                                     (const double3 *)(ctx->d_charges.p + nc), ctx->d_boys.p, S, T,
+                                                     V, 0, om);
+  CUCHK(cudaGetLastError());
+  return CQG_OK;
+}
+
+cqg_status cqg_get_batch_layout(cqg_ctx *ctx, int *nbf_per_mol, long long *offset_per_mol, long long *packed) {
+  if (!ctx) return CQG_ERR_BAD_ARG;
+  for (int m = 0; m < ctx->nmol; ++m) {
+    if (nbf_per_mol) nbf_per_mol[m] = ctx->m_nbf[m];
+    if (offset_per_mol) offset_per_mol[m] = ctx->m_xoff[m];
+  }
+  if (packed) *packed = ctx->packed;
+  return CQG_OK;
+}
+
+cqg_status cqg_twoe_contract_direct_batch(cqg_ctx *ctx, int nmat, const double *const *X, double *const *AX,
+                                          const int *types, const double *scale, const unsigned char *active,
+                                          void *stream) {
+  if (!ctx) return CQG_ERR_BAD_ARG;
+  if (ctx->nshell == 0) {
+    ctx->err = "cqg_set_basis_batch has not been called";
+    return CQG_ERR_STATE;
+  }
+  if (nmat <= 0 || nmat > 8 || !X || !AX || !types || !scale) return CQG_ERR_BAD_ARG;
+  CUCHK(cudaSetDevice(ctx->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  const unsigned char all1 = 1;
+  bool changed = false;
+  for (int m = 0; m < ctx->nmol; ++m) {
+    const unsigned char a = active ? (active[m] ? 1 : 0) : all1;
+    if (a != ctx->h_active[m]) {
+      ctx->h_active[m] = a;
+      changed = true;
+    }
+  }
+  if (changed)
+    CUCHK(cudaMemcpyAsync(ctx->d_active.p, ctx->h_active.data(), ctx->nmol, cudaMemcpyHostToDevice, st));
+  const double *Xg[CQG_MAXG];
+  double *AXg[CQG_MAXG];
+  double sJ[CQG_MAXG], sK[CQG_MAXG];
+  const double *Xu[8];
+  int ng, nxu;
+  cqg_status s = plan_groups(ctx, nmat, X, AX, types, scale, ng, Xg, AXg, sJ, sK, nxu, Xu);
+  if (s != CQG_OK) return s;
+  return contract_device(ctx, ng, Xg, AXg, sJ, sK, nxu, Xu, ctx->max_nbf, ctx->max_nbf, st);
 }
 
 cqg_status cqg_get_stats(cqg_ctx *ctx, cqg_stats *out) {

@@ -76,12 +76,33 @@ __device__ __forceinline__ void boys_eval_rt(int L, double T, const double *__re
   }
 }
 
-__global__ void k_one_e(OneEShells sh, const int2 *__restrict__ pairs, int npairs, int ncharge,
+// Molecule layout for batches: shell -> molecule, per-molecule output offset / leading
+// dimension and charge range.  For one molecule: xoff = 0, ld = caller's, all charges.
+struct OneEMols {
+  const int *shmol;
+  const long long *xoff;
+  const int *nbf;
+  const int *coff;   // charges of molecule m: [coff[m], coff[m+1])
+  int batch;
+};
+
+__global__ void k_one_e(OneEShells sh, const int2 *__restrict__ pairs, long long npairs, int ncharge,
                         const double *__restrict__ Zc, const double3 *__restrict__ Rc,
-                        const double *__restrict__ boys, double *S, double *T, double *V, int ld) {
-  const int ip = blockIdx.x * blockDim.x + threadIdx.x;
+                        const double *__restrict__ boys, double *S0, double *T0, double *V0, int ld, OneEMols om) {
+  const long long ip = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (ip >= npairs) return;
   const int a = pairs[ip].x, b = pairs[ip].y;
+  double *S = S0, *T = T0, *V = V0;
+  int c_beg = 0, c_end = ncharge;
+  if (om.batch) {
+    const int m = om.shmol[a];
+    S += om.xoff[m];
+    T += om.xoff[m];
+    V += om.xoff[m];
+    ld = om.nbf[m];
+    c_beg = om.coff[m];
+    c_end = om.coff[m + 1];
+  }
   const int la = sh.L[a], lb = sh.L[b];
   const int nca = (la + 1) * (la + 2) / 2, ncb = (lb + 1) * (lb + 2) / 2;
   const double3 A = sh.center[a], B = sh.center[b];
@@ -121,7 +142,7 @@ __global__ void k_one_e(OneEShells sh, const int2 *__restrict__ pairs, int npair
         }
       }
       const int Lab = la + lb;
-      for (int c = 0; c < ncharge; ++c) {
+      for (int c = c_beg; c < c_end; ++c) {
         const double3 C = Rc[c];
         const double X = Px - C.x, Y = Py - C.y, Z = Pz - C.z;
         boys_eval_rt(Lab, p * (X * X + Y * Y + Z * Z), boys, F);

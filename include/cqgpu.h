@@ -120,6 +120,28 @@ cqg_status cqg_form_pt(cqg_ctx *ctx, int is_rhf, double xHF, const double *Ps,
 cqg_status cqg_one_e(cqg_ctx *ctx, int ncharge, const double *Z, const double *R, double *S,
                      double *T, double *V, int ld, int on_device, void *stream);
 
+/* ---- Batches: many independent molecules of uneven size in one context ----
+ * cqg_set_basis_batch takes the shells of all molecules concatenated (molecule m has
+ * nshell_per_mol[m] shells).  Matrices of a batch live on the device, packed: molecule m's
+ * nbf_m x nbf_m matrix (leading dimension nbf_m) starts at offset_per_mol[m] (elements)
+ * of one array (cqg_get_batch_layout).  One batched contraction evaluates the quartets of
+ * every active molecule in the same class kernels (one work list per quartet class). */
+cqg_status cqg_set_basis_batch(cqg_ctx *ctx, int nmol, const int *nshell_per_mol, const int *L,
+                               const int *pure, const int *nprim, const double *alpha,
+                               const double *coef, const double *centers);
+cqg_status cqg_get_batch_layout(cqg_ctx *ctx, int *nbf_per_mol, long long *offset_per_mol,
+                                long long *packed);
+/* newTwoEContractDirect for every molecule m with active[m] != 0 (NULL: all), device
+ * pointers to packed matrices; same list semantics as cqg_twoe_contract_direct. */
+cqg_status cqg_twoe_contract_direct_batch(cqg_ctx *ctx, int nmat, const double *const *X,
+                                          double *const *AX, const int *types,
+                                          const double *scale, const unsigned char *active,
+                                          void *stream);
+/* One-electron integrals of every molecule of a batch (charges concatenated per molecule,
+ * ncharge_per_mol[m] of them), into packed device S, T, V. */
+cqg_status cqg_one_e_batch(cqg_ctx *ctx, const int *ncharge_per_mol, const double *Z,
+                           const double *R, double *S, double *T, double *V, void *stream);
+
 /* Statistics of the last contraction (synchronises the context's stream). */
 cqg_status cqg_get_stats(cqg_ctx *ctx, cqg_stats *out);
 /* Largest number of quartets held in the device quartet list at once (8 bytes each;
