@@ -31,6 +31,7 @@ EXPORTED = [
     "cqg_get_sizes", "cqg_twoe_contract_direct", "cqg_form_pt", "cqg_get_stats",
     "cqg_set_timing", "cqg_class_name", "cqg_probe_fma_peak", "cqg_one_e", "cqg_set_list_budget",
     "cqg_set_basis_batch", "cqg_get_batch_layout", "cqg_twoe_contract_direct_batch", "cqg_one_e_batch",
+    "cqg_set_graph_mode", "cqg_graph_status", "cqg_autotune_next", "cqg_get_launch_shapes", "cqg_set_active",
 ]
 
 
@@ -83,6 +84,11 @@ def load(path: str = LIB_PATH):
     L.cqg_twoe_contract_direct_batch.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.POINTER(vp), i, d,
                                                  ctypes.c_char_p, vp]
     L.cqg_one_e_batch.argtypes = [vp, i, d, d, vp, vp, vp, vp]
+    L.cqg_set_graph_mode.argtypes = [vp, ctypes.c_longlong, ctypes.c_int]
+    L.cqg_graph_status.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), i, i, i]
+    L.cqg_autotune_next.argtypes = [vp]
+    L.cqg_get_launch_shapes.argtypes = [vp, i, i]
+    L.cqg_set_active.argtypes = [vp, ctypes.c_char_p]
     L.cqg_class_name.argtypes = [ctypes.c_int]
     L.cqg_class_name.restype = ctypes.c_char_p
     L.cqg_probe_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, d]
@@ -91,7 +97,8 @@ def load(path: str = LIB_PATH):
                  "cqg_get_schwarz", "cqg_get_sizes", "cqg_twoe_contract_direct", "cqg_form_pt",
                  "cqg_get_stats", "cqg_set_timing", "cqg_probe_fma_peak", "cqg_one_e",
                  "cqg_set_list_budget", "cqg_set_basis_batch", "cqg_get_batch_layout",
-                 "cqg_twoe_contract_direct_batch", "cqg_one_e_batch"]:
+                 "cqg_twoe_contract_direct_batch", "cqg_one_e_batch", "cqg_set_graph_mode",
+                 "cqg_graph_status", "cqg_autotune_next", "cqg_get_launch_shapes", "cqg_set_active"]:
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

@@ -98,6 +98,44 @@ class BatchAOIntegrals:
         self.newTwoEContractDirect([Ps, Ps], [PTs, PTs], [0, 1], [1.0, xHF], active)
         return PTs
 
+    # ------------------------------------------------------------------ graphs / tuning ---
+    def set_active(self, active=None):
+        act = None if active is None else bytes(bytearray(1 if a else 0 for a in active))
+        _lib.check(self._L.cqg_set_active(self._ctx, act), self._ctx)
+
+    def enable_graph(self, capacity: int, max_groups: int = 1):
+        """Sync-free contractions with a quartet list of `capacity` entries (0: off)."""
+        _lib.check(self._L.cqg_set_graph_mode(self._ctx, int(capacity), int(max_groups)), self._ctx)
+
+    def graph_status(self):
+        q = ctypes.c_longlong()
+        o, nf, asym = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _lib.check(self._L.cqg_graph_status(self._ctx, ctypes.byref(q), ctypes.byref(o), ctypes.byref(nf),
+                                            ctypes.byref(asym)), self._ctx)
+        return {"quartets": int(q.value), "overflow": bool(o.value), "nonfinite": bool(nf.value),
+                "asymmetric": bool(asym.value)}
+
+    def autotune_next(self):
+        _lib.check(self._L.cqg_autotune_next(self._ctx), self._ctx)
+
+    def launch_shapes(self):
+        cta = np.zeros(110, dtype=np.int32)
+        wpb = np.zeros(110, dtype=np.int32)
+        i = ctypes.POINTER(ctypes.c_int)
+        _lib.check(self._L.cqg_get_launch_shapes(self._ctx, cta.ctypes.data_as(i), wpb.ctypes.data_as(i)), self._ctx)
+        return cta, wpb
+
+    def capture_formPT(self, P_static, PT_static, xHF: float = -0.5):
+        """CUDA graph of one batched RHF Fock build reading P_static, writing PT_static.
+        Graph mode must be on; the call is run once uncaptured first (kernel attributes)."""
+        torch = self.torch
+        self.formPT(P_static, xHF=xHF, PTs=PT_static)
+        torch.cuda.synchronize(self.device)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.formPT(P_static, xHF=xHF, PTs=PT_static)
+        return g
+
     def stats(self):
         s = _lib.CqgStats()
         _lib.check(self._L.cqg_get_stats(self._ctx, ctypes.byref(s)), self._ctx)

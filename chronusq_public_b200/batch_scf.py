@@ -1,0 +1,226 @@
+"""Lock-step RHF SCF for a batch of independent molecules on one GPU.
+
+Every SCF iteration makes ONE batched Fock build for all still-active molecules
+(:class:`~chronusq_public_b200.batch.BatchAOIntegrals`, one work list per quartet class
+shared by all molecules), and does the per-molecule linear algebra in stacks of equally
+sized molecules (batched cuBLAS GEMMs and cuSOLVER ``syevd`` through torch).  The
+iteration itself follows :mod:`chronusq_public_b200.scf` (SAD guess, commutator DIIS,
+damping, the reference's convergence tests), with the energy evaluated for the density the
+Fock matrix was built from, E = Tr(P h) + 1/4 Tr(P PT[P]) + E_nuc.
+"""
+from __future__ import annotations
+
+import time
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from .basis import BasisSet
+from .batch import BatchAOIntegrals
+from .molecule import Molecule
+
+
+class BatchSCF:
+    def __init__(self, molecules: Sequence[Molecule], basis: str, device: int = 0,
+                 thresholdSchwartz: float = 1e-12, ndiis: int = 6):
+        import torch
+        self.torch = torch
+        self.mols = list(molecules)
+        self.bss = [BasisSet(basis, m.atoms, m.coords) for m in self.mols]
+        self.basis_name = basis
+        self.dev = torch.device("cuda", device)
+        self.B = BatchAOIntegrals(self.bss, device=device, thresholdSchwartz=thresholdSchwartz)
+        self.thresh = thresholdSchwartz
+        self.nmol = len(self.mols)
+        self.nocc = []
+        for m in self.mols:
+            if m.nelectrons % 2 or m.mult != 1:
+                raise ValueError("batched SCF is RHF only")
+            self.nocc.append(m.nelectrons // 2)
+        self.ndiis = ndiis
+        self.eneTol = 1e-10
+        self.denTol = 1e-8
+        self.maxSCFIter = 128
+        self.dampParam = 0.1
+        self.Enuc = torch.tensor([m.nuclear_repulsion() for m in self.mols], dtype=torch.float64, device=self.dev)
+        # stacks of equally sized molecules
+        sizes = {}
+        for i, n in enumerate(self.B.nbf):
+            sizes.setdefault(n, []).append(i)
+        self.groups = []
+        for n, members in sorted(sizes.items()):
+            idx = torch.tensor(members, dtype=torch.long, device=self.dev)
+            flat = torch.stack([torch.arange(self.B.offsets[m], self.B.offsets[m] + n * n, device=self.dev)
+                                for m in members])
+            nocc = self.nocc[members[0]]
+            if any(self.nocc[m] != nocc for m in members):
+                raise ValueError("molecules of one size must have the same electron count")
+            self.groups.append({"n": n, "members": members, "idx": idx, "flat": flat, "nocc": nocc})
+        S, T, V = self.B.computeAOOneE(self.mols)
+        self.S, self.H = S, T + V
+        for g in self.groups:
+            Sg = self.gather(S, g)
+            w, U = torch.linalg.eigh(Sg)
+            g["X"] = (U * w.rsqrt().unsqueeze(-2)) @ U.transpose(-1, -2)
+            g["H"] = self.gather(self.H, g)
+            g["S"] = Sg
+
+    # ------------------------------------------------------------------ packing ---
+    def gather(self, packed, g):
+        return packed[g["flat"]].view(-1, g["n"], g["n"])
+
+    def scatter(self, stacked, g, packed):
+        packed[g["flat"].reshape(-1)] = stacked.reshape(-1)
+
+    # ------------------------------------------------------------------ pieces ---
+    def _density(self, FO, g):
+        t = self.torch
+        _, C = t.linalg.eigh(0.5 * FO)
+        Co = C[..., : g["nocc"]]
+        DO = 2.0 * Co @ Co.transpose(-1, -2)
+        return g["X"] @ DO @ g["X"].transpose(-1, -2)
+
+    def sad_density(self):
+        from .scf import atomic_density
+        P = self.B.zeros()
+        cache = {}
+        for m, (mol, bs) in enumerate(zip(self.mols, self.bss)):
+            view = self.B.view(P, m)
+            off = {}
+            o = 0
+            for s in bs.shells:
+                off.setdefault(s.atom, [o, 0])
+                off[s.atom][1] += s.size
+                o += s.size
+            for a, z in enumerate(mol.atoms):
+                if z not in cache:
+                    cache[z] = atomic_density(z, self.basis_name, self.dev.index, self.thresh)[0]
+                b0, nb = off[a]
+                view[b0:b0 + nb, b0:b0 + nb] = cache[z]
+        return P
+
+    # ------------------------------------------------------------------ SCF ---
+    def run(self, density=None, use_graph: bool = False, autotune: bool = False):
+        """Converge every molecule; returns the per-molecule energies (numpy).
+
+        use_graph: the batched Fock build of every iteration is one CUDA-graph replay
+        (captured once, after the guess build).  autotune: the guess build also picks the
+        launch shape of every class work list."""
+        t = self.torch
+        t.cuda.synchronize(self.dev)
+        t0 = time.perf_counter()
+        # guess: SAD superposition -> one batched Fock build -> diagonalise
+        P = self.sad_density() if density is None else density.clone()
+        if autotune:
+            self.B.autotune_next()
+        PT = self.B.formPT(P)
+        graph = None
+        self.graph_replays = 0
+        if use_graph:
+            cap = 2 * self.B.stats()["quartets"] + 4096
+            self.B.enable_graph(cap, 1)
+            P_static, PT_static = P.clone(), self.B.zeros()
+            graph = self.B.capture_formPT(P_static, PT_static)
+        for g in self.groups:
+            F = 2.0 * g["H"] + self.gather(PT, g)
+            self.scatter(self._density(g["X"].transpose(-1, -2) @ F @ g["X"], g), g, P)
+        active = np.ones(self.nmol, dtype=bool)
+        Eold = t.zeros(self.nmol, dtype=t.float64, device=self.dev)
+        energies = t.zeros(self.nmol, dtype=t.float64, device=self.dev)
+        for g in self.groups:
+            g["hist_F"], g["hist_E"] = [], []
+            g["damp"] = t.full((len(g["members"]),), self.dampParam, dtype=t.float64, device=self.dev)
+            g["FO_prev"] = None
+        self.iterations = np.zeros(self.nmol, dtype=int)
+        self.fock_builds = 0
+        self.log = []
+        for it in range(self.maxSCFIter):
+            if graph is not None:
+                self.B.set_active(active.tolist())
+                P_static.copy_(P)
+                graph.replay()
+                st = self.B.graph_status()
+                if st["overflow"]:       # list capacity exceeded: rebuild this one without the graph
+                    self.B.enable_graph(0)
+                    graph = None
+                    PT = self.B.formPT(P, active=active.tolist())
+                else:
+                    PT = PT_static
+                    self.graph_replays += 1
+            else:
+                PT = self.B.formPT(P, active=active.tolist())
+            self.fock_builds += 1
+            Pnew = P.clone()
+            for g in self.groups:
+                gidx = g["idx"]
+                act = t.as_tensor(active[g["members"]], device=self.dev)
+                if not bool(act.any()):
+                    continue
+                Pg = self.gather(P, g)
+                PTg = self.gather(PT, g)
+                E = (Pg * g["H"]).sum((-1, -2)) + 0.25 * (Pg * PTg).sum((-1, -2)) + self.Enuc[gidx]
+                energies[gidx] = t.where(act, E, energies[gidx])
+                F = 2.0 * g["H"] + PTg
+                X = g["X"]
+                FO = X.transpose(-1, -2) @ F @ X
+                Xi = g["S"] @ X          # X^-1 = S^(1/2) = S X for the Loewdin X
+                DO = Xi.transpose(-1, -2) @ Pg @ Xi
+                err = FO @ DO
+                err = err - err.transpose(-1, -2)
+                g["hist_F"].append(F)
+                g["hist_E"].append(err)
+                if len(g["hist_F"]) > self.ndiis:
+                    g["hist_F"].pop(0)
+                    g["hist_E"].pop(0)
+                m = len(g["hist_F"])
+                if m > 1:
+                    Es = t.stack(g["hist_E"], 1).flatten(2)          # (G, m, n^2)
+                    Bm = Es @ Es.transpose(-1, -2)
+                    sc = Bm.diagonal(dim1=-2, dim2=-1).amax(-1).clamp_min(1e-300)
+                    A = t.zeros((Bm.shape[0], m + 1, m + 1), dtype=t.float64, device=self.dev)
+                    A[:, :m, :m] = Bm / sc[:, None, None]
+                    A[:, m, :m] = -1.0
+                    A[:, :m, m] = -1.0
+                    rhs = t.zeros((Bm.shape[0], m + 1), dtype=t.float64, device=self.dev)
+                    rhs[:, m] = -1.0
+                    c = t.linalg.solve(A + 1e-14 * t.eye(m + 1, dtype=t.float64, device=self.dev), rhs)[:, :m]
+                    ok = t.isfinite(c).all(-1) & (c.abs().amax(-1) < 1e6)
+                    Fx = (c[:, :, None, None] * t.stack(g["hist_F"], 1)).sum(1)
+                    F = t.where(ok[:, None, None], Fx, F)
+                    FO = X.transpose(-1, -2) @ F @ X
+                damp = g["damp"]
+                if g["FO_prev"] is not None:
+                    FO = (1.0 - damp)[:, None, None] * FO + damp[:, None, None] * g["FO_prev"]
+                g["FO_prev"] = FO
+                Pn = self._density(FO, g)
+                dE = E - Eold[gidx]
+                dP = (Pn - Pg).flatten(1).norm(dim=-1)
+                Eold[gidx] = t.where(act, E, Eold[gidx])
+                g["damp"] = t.where(dE.abs() < 1e-6, t.zeros_like(damp),
+                                    t.where(damp <= 0.0, t.full_like(damp, self.dampParam), damp))
+                conv = (dE.abs() < self.eneTol) & (dP < self.denTol) & act
+                Pn = t.where(act[:, None, None], Pn, Pg)
+                self.scatter(Pn, g, Pnew)
+                conv_h = conv.cpu().numpy()
+                act_h = act.cpu().numpy()
+                for k, mi in enumerate(g["members"]):
+                    if act_h[k]:
+                        self.iterations[mi] = it + 1
+                    if conv_h[k]:
+                        active[mi] = False
+            P = Pnew
+            t.cuda.synchronize(self.dev)
+            self.log.append((it, int(active.sum()), time.perf_counter() - t0))
+            if not active.any():
+                break
+        if use_graph:
+            self.B.enable_graph(0)
+            self.B.set_active(None)
+        self.seconds = time.perf_counter() - t0
+        self.converged = not active.any()
+        self.energies = energies.cpu().numpy()
+        self.P = P
+        return self.energies
+
+    def close(self):
+        self.B.close()

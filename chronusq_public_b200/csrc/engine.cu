@@ -16,6 +16,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -261,7 +262,7 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
                                                   double cut32, long long *__restrict__ cnt,
                                                   const long long *__restrict__ off, uint2 *__restrict__ qlist,
                                                   unsigned long long *__restrict__ blkacc, long long vt0,
-                                                  long long vt1, long long obase) {
+                                                  long long vt1, long long obase, long long cap) {
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (warp >= ntask) return;
@@ -299,8 +300,14 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
         const bool hi = pass && !lo;
         unsigned b64 = __ballot_sync(0xffffffffu, hi), b32 = __ballot_sync(0xffffffffu, lo);
         const unsigned below = (1u << lane) - 1u;
-        if (FILL && hi && do64) qlist[base64 + c64 + __popc(b64 & below)] = make_uint2((unsigned)bra, (unsigned)ket);
-        if (FILL && lo && do32) qlist[base32 + c32 + __popc(b32 & below)] = make_uint2((unsigned)bra, (unsigned)ket);
+        if (FILL && hi && do64) {
+          const long long pos = base64 + c64 + __popc(b64 & below);
+          if (pos < cap) qlist[pos] = make_uint2((unsigned)bra, (unsigned)ket);
+        }
+        if (FILL && lo && do32) {
+          const long long pos = base32 + c32 + __popc(b32 & below);
+          if (pos < cap) qlist[pos] = make_uint2((unsigned)bra, (unsigned)ket);
+        }
         if (!FILL && hi) {
           km64 += (unsigned long long)P.kk[ket];
           ke64 += (unsigned long long)P.np[ket];
@@ -339,8 +346,10 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
 // Ranges [beg, end) of the quartet list per (precision, class block) from the per-task
 // counts and offsets; virtual block b = prec * nblk + block, prec 0 = FP64, 1 = FP32.
 __global__ void k_block_ranges(BlockTable bt, int ntask, const long long *__restrict__ cnt,
-                               const long long *__restrict__ off, long long *__restrict__ range) {
+                               const long long *__restrict__ off, long long *__restrict__ range, long long cap,
+                               int *__restrict__ flags) {
   int vb = threadIdx.x;
+  if (vb == 0 && ntask > 0 && off[2 * ntask - 1] + cnt[2 * ntask - 1] > cap) flags[2] = 1;   // list overflow
   if (vb >= 2 * bt.nblk) return;
   const int prec = vb / bt.nblk, b = vb % bt.nblk;
   const int t0 = prec * ntask + bt.task_beg[b], t1 = prec * ntask + bt.task_beg[b + 1];
@@ -351,8 +360,8 @@ __global__ void k_block_ranges(BlockTable bt, int ntask, const long long *__rest
   } else if (t0 > 0) {
     beg = end = off[t0 - 1] + cnt[t0 - 1];
   }
-  range[2 * vb] = beg;
-  range[2 * vb + 1] = end;
+  range[2 * vb] = min(beg, cap);
+  range[2 * vb + 1] = min(end, cap);
 }
 
 __device__ __forceinline__ double warp_sum(double x) {
@@ -908,6 +917,14 @@ struct cqg_ctx {
   double fp32_cutoff = 0.0;
   int timing = 0;
   long long list_budget = 1LL << 29;   // quartets held in the list at once (8 B each)
+  int nsm = 148;                       // multiprocessors of the device
+  // launch shapes per (precision, class) work list: persistent CTAs per SM and, for the
+  // warp-cooperative classes, warps per CTA (0 = default); set by the autotuner
+  int shape_cta[2 * CQG_NQC] = {0};
+  int shape_wpb[2 * CQG_NQC] = {0};
+  int autotune_pending = 0;
+  long long graph_capacity = 0;        // > 0: sync-free contraction for CUDA-graph capture
+  bool class_possible[CQG_NQC] = {false};
   // molecules of the context (a batch when nmol > 1)
   int nmol = 0, max_nsh = 0, max_nbf = 0;
   long long packed = 0, Mtotal = 0, nallpairs = 0;
@@ -949,7 +966,7 @@ struct cqg_ctx {
   DevBuf<long long> d_cnt, d_off, d_range;
   DevBuf<unsigned char> d_scan_tmp;
   DevBuf<uint2> d_qlist;
-  DevBuf<double> d_G, d_X, d_AX;
+  DevBuf<double> d_G, d_X, d_AX, d_Gscratch;
   BlockTable bt;
   int ntask = 0;
   cudaEvent_t ev[4 + 2 * 55];
@@ -985,18 +1002,22 @@ __host__ __device__ constexpr bool is_warp_class(int la, int lb, int lc, int ld)
 template <int LA, int LB, int LC, int LD, bool SCHWARZ, typename T>
 static cudaError_t launch_warp(cqg_ctx *ctx, int blk, long long n, long long sbeg, long long send, cudaStream_t st,
                                const DigestGroups &dg, double *Q) {
-  if (n <= 0) return cudaSuccess;
+  if (n == 0) return cudaSuccess;   // n < 0: count unknown on the host (graph mode)
   static bool attr_set = false;
   const size_t per_warp = warp_smem_bytes<LA, LB, LC, LD, T>() / 4;
-  const int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (200u * 1024u) / per_warp));
-  const size_t smem = per_warp * wpb;
+  const int wpb_max = (int)std::max<size_t>(1, std::min<size_t>(4, (200u * 1024u) / per_warp));
   if (!attr_set) {
     cudaError_t e = cudaFuncSetAttribute(k_eri_jk_warp<LA, LB, LC, LD, SCHWARZ, T>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(per_warp * wpb_max));
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
-  const int blocks = (int)std::min<long long>((n + wpb - 1) / wpb, 148LL * 16);
+  int wpb = wpb_max, cta = 16;
+  if (!SCHWARZ && ctx->shape_wpb[blk] > 0) wpb = std::min(wpb_max, ctx->shape_wpb[blk]);
+  if (!SCHWARZ && ctx->shape_cta[blk] > 0) cta = ctx->shape_cta[blk];
+  const size_t smem = per_warp * wpb;
+  const long long cap = (long long)ctx->nsm * cta;
+  const int blocks = (int)(n > 0 ? std::min<long long>((n + wpb - 1) / wpb, cap) : cap);
   k_eri_jk_warp<LA, LB, LC, LD, SCHWARZ, T><<<blocks, 32 * wpb, smem, st>>>(ctx->d_qlist.p, ctx->d_range.p, blk, sbeg,
                                                                        send, make_pairs(ctx), make_shells(ctx),
                                                                        ctx->d_boys.p, dg, Q);
@@ -1120,11 +1141,13 @@ typedef cudaError_t (*eri_launcher)(cqg_ctx *, int blk, long long n, cudaStream_
 
 template <int LA, int LB, int LC, int LD, typename T>
 static cudaError_t launch_eri(cqg_ctx *ctx, int blk, long long n, cudaStream_t st, const DigestGroups &dg) {
-  if (n <= 0) return cudaSuccess;
+  if (n == 0) return cudaSuccess;   // n < 0: count unknown on the host (graph mode)
   if constexpr (is_warp_class(LA, LB, LC, LD)) {
     return launch_warp<LA, LB, LC, LD, false, T>(ctx, blk, n, 0, 0, st, dg, nullptr);
   } else {
-    long long nb = std::min<long long>((n + 127) / 128, 148LL * 12);
+    const int cta = ctx->shape_cta[blk] > 0 ? ctx->shape_cta[blk] : 12;
+    const long long cap = (long long)ctx->nsm * cta;
+    long long nb = n > 0 ? std::min<long long>((n + 127) / 128, cap) : cap;
     k_eri_jk<LA, LB, LC, LD, T><<<(unsigned)nb, 128, 0, st>>>(ctx->d_qlist.p, ctx->d_range.p, blk, make_pairs(ctx),
                                                            make_shells(ctx), ctx->d_boys.p, dg);
     return cudaGetLastError();
@@ -1190,6 +1213,7 @@ cqg_status cqg_create(cqg_ctx **out, int device) {
   }
   for (int i = 0; i < 4 + 2 * 55; ++i) cudaEventCreate(&ctx->ev[i]);
   ctx->events = true;
+  cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
   *out = ctx;
   return CQG_OK;
 }
@@ -1207,7 +1231,7 @@ cqg_status cqg_destroy(cqg_ctx *ctx) {
   ctx->d_prim.release(); ctx->d_boys.release();
   ctx->d_M.release(); ctx->d_Mmax.release(); ctx->d_flags.release();
   ctx->d_cnt.release(); ctx->d_off.release(); ctx->d_range.release(); ctx->d_scan_tmp.release();
-  ctx->d_qlist.release(); ctx->d_G.release(); ctx->d_X.release(); ctx->d_AX.release();
+  ctx->d_qlist.release(); ctx->d_G.release(); ctx->d_X.release(); ctx->d_AX.release(); ctx->d_Gscratch.release();
   if (ctx->events)
     for (int i = 0; i < 4 + 2 * 55; ++i) cudaEventDestroy(ctx->ev[i]);
   delete ctx;
@@ -1482,6 +1506,11 @@ cqg_status cqg_set_basis_batch(cqg_ctx *ctx, int nmol, const int *nshell_per_mol
   bt.task_beg[CQG_NQC] = task;
   bt.nblk = CQG_NQC;
   ctx->ntask = task;
+  for (int k = 0; k < CQG_NQC; ++k) {
+    int i, j;
+    qclass_split(k, i, j);
+    ctx->class_possible[k] = ctx->pc_beg[i + 1] > ctx->pc_beg[i] && ctx->pc_beg[j + 1] > ctx->pc_beg[j];
+  }
   size_t scan_bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (long long *)nullptr, (long long *)nullptr, std::max(2 * task, 1));
   if (ctx->d_cnt.reserve(2 * task + 1) || ctx->d_off.reserve(2 * task + 1) || ctx->d_range.reserve(4 * CQG_NQC) ||
@@ -1500,6 +1529,145 @@ cqg_status cqg_get_schwarz(cqg_ctx *ctx, double *Q) {
   if (!ctx || !Q) return CQG_ERR_BAD_ARG;
   if (ctx->nshell == 0) return CQG_ERR_STATE;
   memcpy(Q, ctx->Qmat.data(), ctx->Qmat.size() * sizeof(double));
+  return CQG_OK;
+}
+
+// Launch-shape autotuner: for every (precision, class) list with work, time each candidate
+// shape (persistent CTAs per SM; warps per CTA for the warp-cooperative classes) with the
+// digest pointed at scratch accumulators, and keep the fastest.
+static cqg_status autotune_shapes(cqg_ctx *ctx, const long long *crange, cudaStream_t st, const DigestGroups &dg) {
+  DigestGroups scratch = dg;
+  size_t per = 0;
+  for (int g = 0; g < dg.ng; ++g) per = std::max<size_t>(per, 1);
+  const size_t gsize = ctx->nmol > 1 ? (size_t)ctx->packed : (size_t)ctx->nbf * ctx->nbf;
+  if (ctx->d_Gscratch.reserve(gsize) != cudaSuccess) return CQG_ERR_OOM;
+  for (int g = 0; g < dg.ng; ++g) scratch.G[g] = ctx->d_Gscratch.p;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (int vb = 0; vb < 2 * CQG_NQC; ++vb) {
+    const long long n = crange[2 * vb + 1] - crange[2 * vb];
+    if (n <= 0) continue;
+    const int k = vb % CQG_NQC;
+    int i, j;
+    qclass_split(k, i, j);
+    const bool warp = is_warp_class(kPairClass[i][0], kPairClass[i][1], kPairClass[j][0], kPairClass[j][1]);
+    std::vector<std::pair<int, int>> cand;   // (cta per SM, warps per CTA)
+    if (warp) {
+      for (int w : {1, 2, 4})
+        for (int c : {8, 16, 32}) cand.push_back({c, w});
+    } else {
+      for (int c : {4, 8, 12, 16, 24}) cand.push_back({c, 0});
+    }
+    float best = 1e30f;
+    std::pair<int, int> pick = cand[0];
+    for (auto &cw : cand) {
+      ctx->shape_cta[vb] = cw.first;
+      ctx->shape_wpb[vb] = cw.second;
+      float tbest = 1e30f;
+      for (int rep = 0; rep < 2; ++rep) {
+        cudaEventRecord(e0, st);
+        cudaError_t e = (vb < CQG_NQC ? kEriLaunch[k] : kEriLaunch32[k])(ctx, vb, n, st, scratch);
+        cudaEventRecord(e1, st);
+        if (e != cudaSuccess) {
+          cudaEventDestroy(e0);
+          cudaEventDestroy(e1);
+          ctx->err = std::string("autotune launch: ") + cudaGetErrorString(e);
+          return CQG_ERR_CUDA;
+        }
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        tbest = std::min(tbest, ms);
+      }
+      if (tbest < best) {
+        best = tbest;
+        pick = cw;
+      }
+    }
+    ctx->shape_cta[vb] = pick.first;
+    ctx->shape_wpb[vb] = pick.second;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return CQG_OK;
+}
+
+// Sync-free contraction for CUDA-graph capture: the quartet list has a fixed capacity,
+// every class kernel reads its range from device memory and runs a persistent grid, and
+// nothing is read back.  Overflow of the capacity and invalid inputs are reported through
+// device flags (cqg_graph_status).
+static cqg_status contract_graph(cqg_ctx *ctx, int ngroups, const double *const *Xg, double *const *AXg,
+                                 const double *sJ, const double *sK, int nx_all, const double *const *Xall, int ldx,
+                                 int ldax, cudaStream_t st) {
+  const Mols mols = make_mols(ctx);
+  const size_t gsize = ctx->nmol > 1 ? (size_t)ctx->packed : (size_t)ctx->nbf * ctx->nbf;
+  if ((size_t)ngroups * gsize > ctx->d_G.n || (size_t)ctx->graph_capacity > ctx->d_qlist.n) {
+    ctx->err = "graph mode: buffers were not reserved for this call (cqg_set_graph_mode)";
+    return CQG_ERR_STATE;
+  }
+  XList xl;
+  xl.n = nx_all;
+  for (int i = 0; i < nx_all; ++i) xl.X[i] = Xall[i];
+  const double cut32 = ctx->policy == CQG_PREC_MIXED ? ctx->fp32_cutoff : 0.0;
+  CUCHK(cudaMemsetAsync(ctx->d_flags.p, 0, 4 * sizeof(int), st));
+  CUCHK(cudaMemsetAsync(ctx->d_Mmax.p, 0, sizeof(double), st));
+  CUCHK(cudaMemsetAsync(ctx->d_blkacc.p, 0, 4 * CQG_NQC * sizeof(unsigned long long), st));
+  CUCHK(cudaMemsetAsync(ctx->d_G.p, 0, (size_t)ngroups * gsize * sizeof(double), st));
+  {
+    dim3 g((ctx->max_nsh + 127) / 128, ctx->max_nsh, ctx->nmol);
+    k_blocknorm<<<g, 128, 0, st>>>(xl, ldx, mols, ctx->d_bf.p, ctx->d_sz.p, ctx->d_M.p, ctx->d_flags.p, 1e-12);
+    const long long nn = ctx->Mtotal;
+    k_maxreduce<<<(int)std::min<long long>((nn + 255) / 256, 1184), 256, 0, st>>>(ctx->d_M.p, nn, ctx->d_Mmax.p);
+  }
+  Pairs P = make_pairs(ctx);
+  const int nb = (ctx->ntask + 7) / 8;
+  k_quartets<false><<<nb, 256, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
+                                         ctx->thresh, cut32, ctx->d_cnt.p, nullptr, nullptr, ctx->d_blkacc.p, 0, 0, 0,
+                                         0);
+  size_t scan_bytes = ctx->d_scan_tmp.n;
+  CUCHK(cub::DeviceScan::ExclusiveSum(ctx->d_scan_tmp.p, scan_bytes, ctx->d_cnt.p, ctx->d_off.p, 2 * ctx->ntask, st));
+  k_block_ranges<<<1, 128, 0, st>>>(ctx->bt, ctx->ntask, ctx->d_cnt.p, ctx->d_off.p, ctx->d_range.p,
+                                    ctx->graph_capacity, ctx->d_flags.p);
+  k_quartets<true><<<nb, 256, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
+                                        ctx->thresh, cut32, nullptr, ctx->d_off.p, ctx->d_qlist.p, nullptr, 0,
+                                        2LL * ctx->ntask, 0, ctx->graph_capacity);
+  CUCHK(cudaGetLastError());
+  DigestGroups dg;
+  memset(&dg, 0, sizeof(dg));
+  dg.ng = ngroups;
+  dg.ldx = ldx;
+  dg.batch = ctx->nmol > 1;
+  dg.xoff = ctx->d_mxoff.p;
+  dg.nbf = ctx->d_mnbf.p;
+  for (int g = 0; g < ngroups; ++g) {
+    dg.X[g] = Xg[g];
+    dg.G[g] = ctx->d_G.p + (size_t)g * gsize;
+    dg.sJ[g] = sJ[g];
+    dg.sK[g] = sK[g];
+  }
+  int launches = 6;
+  for (int k = 0; k < CQG_NQC; ++k) {
+    if (!ctx->class_possible[k]) continue;
+    cudaError_t e = kEriLaunch[k](ctx, k, -1, st, dg);
+    ++launches;
+    if (e == cudaSuccess && ctx->policy == CQG_PREC_MIXED) {
+      e = kEriLaunch32[k](ctx, CQG_NQC + k, -1, st, dg);
+      ++launches;
+    }
+    if (e != cudaSuccess) {
+      ctx->err = std::string("eri kernel ") + cqg_class_name(k) + ": " + cudaGetErrorString(e);
+      return CQG_ERR_CUDA;
+    }
+  }
+  for (int g = 0; g < ngroups; ++g) {
+    dim3 grid((ctx->max_nbf + 31) / 32, (ctx->max_nbf + 31) / 32, ctx->nmol), blk(32, 8);
+    k_finalize<<<grid, blk, 0, st>>>(dg.G[g], mols, AXg[g], ldax);
+    ++launches;
+  }
+  CUCHK(cudaGetLastError());
+  ctx->launches = launches;
+  ctx->stats.launches = launches;
   return CQG_OK;
 }
 
@@ -1537,11 +1705,12 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     int nb = (ctx->ntask + wpb - 1) / wpb;
     k_quartets<false><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
                                             ctx->thresh,
-                                            cut32, ctx->d_cnt.p, nullptr, nullptr, ctx->d_blkacc.p, 0, 0, 0);
+                                            cut32, ctx->d_cnt.p, nullptr, nullptr, ctx->d_blkacc.p, 0, 0, 0, 0);
     CUCHK(cudaGetLastError());
     size_t scan_bytes = ctx->d_scan_tmp.n;
     CUCHK(cub::DeviceScan::ExclusiveSum(ctx->d_scan_tmp.p, scan_bytes, ctx->d_cnt.p, ctx->d_off.p, 2 * ctx->ntask, st));
-    k_block_ranges<<<1, 128, 0, st>>>(ctx->bt, ctx->ntask, ctx->d_cnt.p, ctx->d_off.p, ctx->d_range.p);
+    k_block_ranges<<<1, 128, 0, st>>>(ctx->bt, ctx->ntask, ctx->d_cnt.p, ctx->d_off.p, ctx->d_range.p, LLONG_MAX,
+                                      ctx->d_flags.p);
     CUCHK(cudaGetLastError());
     ctx->launches += 2;
   }
@@ -1659,11 +1828,17 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
       int nb = (ctx->ntask + wpb - 1) / wpb;
       k_quartets<true><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
                                              ctx->thresh,
-                                             cut32, nullptr, ctx->d_off.p, ctx->d_qlist.p, nullptr, vt0, vt1, obase);
+                                             cut32, nullptr, ctx->d_off.p, ctx->d_qlist.p, nullptr, vt0, vt1, obase,
+                                             (long long)ctx->d_qlist.n);
       CUCHK(cudaGetLastError());
       ctx->launches += 1;
     }
     if (ctx->timing && first_chunk) CUCHK(cudaEventRecord(ctx->ev[1], st));
+    if (ctx->autotune_pending && chunk_vt.size() == 2) {
+      cqg_status ts = autotune_shapes(ctx, crange, st, dg);
+      if (ts != CQG_OK) return ts;
+      ctx->autotune_pending = 0;
+    }
     // 3. ERI + digest per class
     for (int k = 0; k < CQG_NQC; ++k) {
       const long long n64 = crange[2 * k + 1] - crange[2 * k];
@@ -1765,6 +1940,7 @@ cqg_status cqg_twoe_contract_direct(cqg_ctx *ctx, int nmat, const double *const 
   cqg_status s = plan_groups(ctx, nmat, X, AX, types, scale, ng, Xg, AXg, sJ, sK, nxu, Xu);
   if (s != CQG_OK) return s;
   const int n = ctx->nbf;
+  if (on_device && ctx->graph_capacity > 0) return contract_graph(ctx, ng, Xg, AXg, sJ, sK, nxu, Xu, ld, ld, st);
   if (on_device) return contract_device(ctx, ng, Xg, AXg, sJ, sK, nxu, Xu, ld, ld, st);
   // host pointers: stage distinct X and each group's AX on the device
   size_t nn = (size_t)n * n;
@@ -1956,6 +2132,10 @@ cqg_status cqg_twoe_contract_direct_batch(cqg_ctx *ctx, int nmat, const double *
       changed = true;
     }
   }
+  if (changed && ctx->graph_capacity > 0) {
+    ctx->err = "graph mode: change the active set with cqg_set_active outside the captured call";
+    return CQG_ERR_STATE;
+  }
   if (changed)
     CUCHK(cudaMemcpyAsync(ctx->d_active.p, ctx->h_active.data(), ctx->nmol, cudaMemcpyHostToDevice, st));
   const double *Xg[CQG_MAXG];
@@ -1965,7 +2145,62 @@ cqg_status cqg_twoe_contract_direct_batch(cqg_ctx *ctx, int nmat, const double *
   int ng, nxu;
   cqg_status s = plan_groups(ctx, nmat, X, AX, types, scale, ng, Xg, AXg, sJ, sK, nxu, Xu);
   if (s != CQG_OK) return s;
+  if (ctx->graph_capacity > 0) return contract_graph(ctx, ng, Xg, AXg, sJ, sK, nxu, Xu, ctx->max_nbf, ctx->max_nbf, st);
   return contract_device(ctx, ng, Xg, AXg, sJ, sK, nxu, Xu, ctx->max_nbf, ctx->max_nbf, st);
+}
+
+cqg_status cqg_set_graph_mode(cqg_ctx *ctx, long long capacity, int max_groups) {
+  if (!ctx || capacity < 0 || max_groups < 0 || max_groups > CQG_MAXG) return CQG_ERR_BAD_ARG;
+  if (ctx->nshell == 0) return CQG_ERR_STATE;
+  CUCHK(cudaSetDevice(ctx->device));
+  ctx->graph_capacity = capacity;
+  if (capacity > 0) {
+    const size_t gsize = ctx->nmol > 1 ? (size_t)ctx->packed : (size_t)ctx->nbf * ctx->nbf;
+    if (ctx->d_qlist.reserve((size_t)capacity) || ctx->d_G.reserve((size_t)std::max(max_groups, 1) * gsize)) {
+      ctx->graph_capacity = 0;
+      return CQG_ERR_OOM;
+    }
+  }
+  return CQG_OK;
+}
+
+cqg_status cqg_graph_status(cqg_ctx *ctx, long long *quartets, int *overflow, int *nonfinite, int *asymmetric) {
+  if (!ctx) return CQG_ERR_BAD_ARG;
+  CUCHK(cudaSetDevice(ctx->device));
+  CUCHK(cudaDeviceSynchronize());
+  long long hr[4 * CQG_NQC];
+  int fl[4];
+  CUCHK(cudaMemcpy(fl, ctx->d_flags.p, sizeof(fl), cudaMemcpyDeviceToHost));
+  CUCHK(cudaMemcpy(hr, ctx->d_range.p, sizeof(hr), cudaMemcpyDeviceToHost));
+  if (quartets) *quartets = hr[4 * CQG_NQC - 1];
+  if (overflow) *overflow = fl[2];
+  if (nonfinite) *nonfinite = fl[0];
+  if (asymmetric) *asymmetric = fl[1];
+  return CQG_OK;
+}
+
+cqg_status cqg_set_active(cqg_ctx *ctx, const unsigned char *active) {
+  if (!ctx) return CQG_ERR_BAD_ARG;
+  if (ctx->nshell == 0) return CQG_ERR_STATE;
+  CUCHK(cudaSetDevice(ctx->device));
+  for (int m = 0; m < ctx->nmol; ++m) ctx->h_active[m] = active ? (active[m] ? 1 : 0) : 1;
+  CUCHK(cudaMemcpy(ctx->d_active.p, ctx->h_active.data(), ctx->nmol, cudaMemcpyHostToDevice));
+  return CQG_OK;
+}
+
+cqg_status cqg_autotune_next(cqg_ctx *ctx) {
+  if (!ctx) return CQG_ERR_BAD_ARG;
+  ctx->autotune_pending = 1;
+  return CQG_OK;
+}
+
+cqg_status cqg_get_launch_shapes(cqg_ctx *ctx, int *cta_per_sm, int *warps_per_cta) {
+  if (!ctx) return CQG_ERR_BAD_ARG;
+  for (int k = 0; k < 2 * CQG_NQC; ++k) {
+    if (cta_per_sm) cta_per_sm[k] = ctx->shape_cta[k];
+    if (warps_per_cta) warps_per_cta[k] = ctx->shape_wpb[k];
+  }
+  return CQG_OK;
 }
 
 cqg_status cqg_get_stats(cqg_ctx *ctx, cqg_stats *out) {

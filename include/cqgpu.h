@@ -142,6 +142,28 @@ cqg_status cqg_twoe_contract_direct_batch(cqg_ctx *ctx, int nmat, const double *
 cqg_status cqg_one_e_batch(cqg_ctx *ctx, const int *ncharge_per_mol, const double *Z,
                            const double *R, double *S, double *T, double *V, void *stream);
 
+/* ---- CUDA graphs and launch shapes ----
+ * cqg_set_graph_mode(ctx, capacity, max_groups): capacity > 0 makes device-pointer
+ * contractions free of host synchronisation so they can be captured in a CUDA graph and
+ * replayed (one graph per SCF iteration shape).  The quartet list holds at most `capacity`
+ * quartets and up to `max_groups` distinct (X, AX) pairs are allowed per call; after a
+ * replay, cqg_graph_status reports the screened quartet count and whether the capacity
+ * overflowed (the result is then incomplete and must be recomputed with a larger
+ * capacity) or the input was non-finite / asymmetric.  capacity = 0 restores the default.
+ * Per-class statistics are not collected in graph mode. */
+cqg_status cqg_set_graph_mode(cqg_ctx *ctx, long long capacity, int max_groups);
+cqg_status cqg_graph_status(cqg_ctx *ctx, long long *quartets, int *overflow, int *nonfinite,
+                            int *asymmetric);
+/* Autotuner: the next (non-graph, single-chunk) contraction times every candidate launch
+ * shape of each class work list (persistent CTAs per SM; warps per CTA for the
+ * warp-cooperative classes) and keeps the fastest for later calls.  The shapes are read
+ * back with cqg_get_launch_shapes (2 x 55 entries: FP64 lists then FP32 lists; 0 = default). */
+cqg_status cqg_autotune_next(cqg_ctx *ctx);
+/* Set which molecules of a batch take part in the following contractions (NULL: all);
+ * a synchronous copy, to be called outside any captured region. */
+cqg_status cqg_set_active(cqg_ctx *ctx, const unsigned char *active);
+cqg_status cqg_get_launch_shapes(cqg_ctx *ctx, int *cta_per_sm, int *warps_per_cta);
+
 /* Statistics of the last contraction (synchronises the context's stream). */
 cqg_status cqg_get_stats(cqg_ctx *ctx, cqg_stats *out);
 /* Largest number of quartets held in the device quartet list at once (8 bytes each;
