@@ -258,6 +258,9 @@ def main():
     ap.add_argument("--fp32-cutoff", type=float, default=1e-8)
     ap.add_argument("--sweep", action="store_true", help="also sweep the FP32 cutoff 1e-10..1e-6")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="also run the batched-SCF comparison on this many (H2O)_n, n in 1..24, 6-31G(d)")
+    ap.add_argument("--batch-single", type=int, default=64, help="molecules converged one at a time")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     if args.impl == "reference":
@@ -371,6 +374,9 @@ def main():
         if not args.no_scf:
             line["scf"] = scf_compare(mol, bs, w["thresh"], args.fp32_cutoff,
                                       sweep=(1e-10, 1e-9, 1e-8, 1e-7, 1e-6) if args.sweep else ())
+        if args.batch > 0:
+            from chronusq_public_b200.workloads import batch_scf_comparison
+            line["batch_scf"] = batch_scf_comparison(args.batch, args.batch_single)
         if not args.no_cpu_baseline and ws == 1:
             line["cpu_baseline"] = cpu_baseline(bs, D, w["thresh"], target_s=args.ref_seconds)
         print(json.dumps(line), flush=True)

@@ -116,11 +116,16 @@ class BatchSCF:
         PT = self.B.formPT(P)
         graph = None
         self.graph_replays = 0
+        self.graph_captures = 0
         if use_graph:
+            free, _ = t.cuda.mem_get_info(self.dev)
+            self.graph_memory_limit = 0.4 * free
             cap = 2 * self.B.stats()["quartets"] + 4096
-            self.B.enable_graph(cap, 1)
-            P_static, PT_static = P.clone(), self.B.zeros()
-            graph = self.B.capture_formPT(P_static, PT_static)
+            if cap * 8 <= self.graph_memory_limit:
+                self.B.enable_graph(cap, 1)
+                P_static, PT_static = P.clone(), self.B.zeros()
+                graph = self.B.capture_formPT(P_static, PT_static)
+                self.graph_captures = 1
         for g in self.groups:
             F = 2.0 * g["H"] + self.gather(PT, g)
             self.scatter(self._density(g["X"].transpose(-1, -2) @ F @ g["X"], g), g, P)
@@ -140,10 +145,20 @@ class BatchSCF:
                 P_static.copy_(P)
                 graph.replay()
                 st = self.B.graph_status()
-                if st["overflow"]:       # list capacity exceeded: rebuild this one without the graph
+                if st["overflow"]:
+                    # the list capacity was sized on the guess build: rebuild this iteration
+                    # without the graph, then recapture with room for this density's quartets
                     self.B.enable_graph(0)
-                    graph = None
+                    self.B.set_active(None)
                     PT = self.B.formPT(P, active=active.tolist())
+                    need = int(1.25 * self.B.stats()["quartets"]) + 4096
+                    graph = None
+                    if need * 8 <= self.graph_memory_limit:
+                        self.B.set_active(None)
+                        self.B.enable_graph(need, 1)
+                        P_static.copy_(P)
+                        graph = self.B.capture_formPT(P_static, PT_static)
+                        self.graph_captures += 1
                 else:
                     PT = PT_static
                     self.graph_replays += 1

@@ -916,7 +916,7 @@ struct cqg_ctx {
   int policy = CQG_PREC_FP64;
   double fp32_cutoff = 0.0;
   int timing = 0;
-  long long list_budget = 1LL << 29;   // quartets held in the list at once (8 B each)
+  long long list_budget = 1LL << 32;   // quartets held in the list at once (8 B each: 32 GiB)
   int nsm = 148;                       // multiprocessors of the device
   // launch shapes per (precision, class) work list: persistent CTAs per SM and, for the
   // warp-cooperative classes, warps per CTA (0 = default); set by the autotuner

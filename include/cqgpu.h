@@ -167,7 +167,7 @@ cqg_status cqg_get_launch_shapes(cqg_ctx *ctx, int *cta_per_sm, int *warps_per_c
 /* Statistics of the last contraction (synchronises the context's stream). */
 cqg_status cqg_get_stats(cqg_ctx *ctx, cqg_stats *out);
 /* Largest number of quartets held in the device quartet list at once (8 bytes each;
- * default 2^29).  Larger screened sets are filled and evaluated in chunks. */
+ * default 2^32, 32 GiB).  Larger screened sets are filled and evaluated in chunks. */
 cqg_status cqg_set_list_budget(cqg_ctx *ctx, long long quartets);
 /* Per-class kernel timing on (1) / off (0, default). */
 cqg_status cqg_set_timing(cqg_ctx *ctx, int on);
