@@ -32,6 +32,7 @@ EXPORTED = [
     "cqg_set_timing", "cqg_class_name", "cqg_probe_fma_peak", "cqg_one_e", "cqg_set_list_budget",
     "cqg_set_basis_batch", "cqg_get_batch_layout", "cqg_twoe_contract_direct_batch", "cqg_one_e_batch",
     "cqg_set_graph_mode", "cqg_graph_status", "cqg_autotune_next", "cqg_get_launch_shapes", "cqg_set_active",
+    "cqg_mlp_gemm_bf16", "cqg_mlp_silu_bwd", "cqg_mlp_to_bf16", "cqg_mlp_colsum", "cqg_mlp_mse", "cqg_mlp_adam",
 ]
 
 
@@ -89,6 +90,14 @@ def load(path: str = LIB_PATH):
     L.cqg_autotune_next.argtypes = [vp]
     L.cqg_get_launch_shapes.argtypes = [vp, i, i]
     L.cqg_set_active.argtypes = [vp, ctypes.c_char_p]
+    ll, f, fp = ctypes.c_longlong, ctypes.c_float, ctypes.POINTER(ctypes.c_float)
+    L.cqg_mlp_gemm_bf16.argtypes = [vp, ll, ll, vp, ll, ll, vp, ll, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp,
+                                    vp, ll, ctypes.c_int, ctypes.c_int, vp]
+    L.cqg_mlp_silu_bwd.argtypes = [vp, vp, vp, ll, vp]
+    L.cqg_mlp_to_bf16.argtypes = [vp, vp, ll, vp]
+    L.cqg_mlp_colsum.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp]
+    L.cqg_mlp_mse.argtypes = [vp, vp, vp, ll, f, vp, vp, vp]
+    L.cqg_mlp_adam.argtypes = [vp, vp, vp, vp, ll, f, f, f, f, ctypes.c_int, f, vp, vp]
     L.cqg_class_name.argtypes = [ctypes.c_int]
     L.cqg_class_name.restype = ctypes.c_char_p
     L.cqg_probe_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, d]
@@ -98,7 +107,9 @@ def load(path: str = LIB_PATH):
                  "cqg_get_stats", "cqg_set_timing", "cqg_probe_fma_peak", "cqg_one_e",
                  "cqg_set_list_budget", "cqg_set_basis_batch", "cqg_get_batch_layout",
                  "cqg_twoe_contract_direct_batch", "cqg_one_e_batch", "cqg_set_graph_mode",
-                 "cqg_graph_status", "cqg_autotune_next", "cqg_get_launch_shapes", "cqg_set_active"]:
+                 "cqg_graph_status", "cqg_autotune_next", "cqg_get_launch_shapes", "cqg_set_active",
+                 "cqg_mlp_gemm_bf16", "cqg_mlp_silu_bwd", "cqg_mlp_to_bf16", "cqg_mlp_colsum", "cqg_mlp_mse",
+                 "cqg_mlp_adam"]:
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

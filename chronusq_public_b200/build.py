@@ -48,7 +48,8 @@ def build(force: bool = False, verbose: bool = True) -> str:
         return OUT
     os.makedirs(os.path.dirname(GEN), exist_ok=True)
     subprocess.check_call([sys.executable, os.path.join(CSRC, "gen_eri.py"), GEN, str(MAXL)])
-    cmd = [_nvcc()] + NVCC_FLAGS + ["-o", OUT + ".tmp", os.path.join(CSRC, "engine.cu")]
+    cmd = [_nvcc()] + NVCC_FLAGS + ["-o", OUT + ".tmp", os.path.join(CSRC, "engine.cu"),
+                                    os.path.join(CSRC, "mlp.cu")]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.check_call(cmd)

@@ -174,6 +174,28 @@ cqg_status cqg_set_timing(cqg_ctx *ctx, int on);
 /* Name of quartet class index k ("(pp|ps)"), or NULL past the last class. */
 const char *cqg_class_name(int k);
 
+/* ---- Kernels of the learned initial-density model (csrc/mlp.cu) ----
+ * BF16 operands, FP32 accumulation; all pointers are device pointers, work is enqueued on
+ * `stream`.  cqg_mlp_gemm_bf16: C(m,n) (+)= sum_k A[m*sam + k*sak] * B[n*sbn + k*sbk]
+ * (accumulate != 0 adds into C), then if bias: C += bias[n]; if Y: Y = act ? SiLU(C) : C
+ * in BF16 (leading dimension ldy).  cqg_mlp_silu_bwd: dZ = dY * SiLU'(Z) (BF16).
+ * cqg_mlp_colsum: db[n] = sum_m dZ[m][n].  cqg_mlp_mse: *loss += sum mask (p-t)^2 * inv_count,
+ * dpred = 2 mask (p-t) inv_count.  cqg_mlp_adam: one Adam step (bias-corrected, decoupled
+ * weight decay folded into the gradient) on FP32 weights, optional BF16 copy.
+ * These have no counterpart in the reference (it has no learned guess). */
+cqg_status cqg_mlp_gemm_bf16(const void *A, long long sam, long long sak, const void *B,
+                             long long sbn, long long sbk, float *C, long long ldc, int M, int N,
+                             int K, const float *bias, void *Y, long long ldy, int act,
+                             int accumulate, void *stream);
+cqg_status cqg_mlp_silu_bwd(const float *dY, const float *Z, void *dZ, long long n, void *stream);
+cqg_status cqg_mlp_to_bf16(const float *x, void *y, long long n, void *stream);
+cqg_status cqg_mlp_colsum(const void *dZ, int M, int N, float *db, void *stream);
+cqg_status cqg_mlp_mse(const float *pred, const float *target, const float *mask, long long n,
+                       float inv_count, float *dpred, float *loss, void *stream);
+cqg_status cqg_mlp_adam(float *w, const float *g, float *m1, float *m2, long long n, float lr,
+                        float b1, float b2, float eps, int step, float weight_decay, void *wbf,
+                        void *stream);
+
 /* FP64 / FP32 FMA throughput probe used to report roofline fractions: runs a dependent
  * FMA chain kernel for `ms_target` ms and returns achieved TFLOP/s in *tflops. */
 cqg_status cqg_probe_fma_peak(int device, int fp64, double ms_target, double *tflops);
