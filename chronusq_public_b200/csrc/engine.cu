@@ -2254,3 +2254,81 @@ cqg_status cqg_probe_fma_peak(int device, int fp64, double ms_target, double *tf
 }
 
 }  // extern "C"
+
+// ---- One-electron integrals that allocate nothing ---------------------------------------
+// The point-charge table lives in a fixed module-scope device array instead of the
+// context's growable buffer; its device address is resolved once per device.
+#include <mutex>
+
+namespace {
+constexpr int kNoAllocMaxDevices = 64;
+// Z[0..n) followed by R[n..4n) (x, y, z per charge), as k_one_e reads it
+__device__ __align__(256) double g_oe_charge_table[4 * CQG_ONE_E_NOALLOC_MAX_CHARGES];
+std::mutex g_oe_table_mutex;
+double *g_oe_table_addr[kNoAllocMaxDevices] = {};
+
+// With ctx->device current: the device address of g_oe_charge_table on that device.
+cqg_status oe_charge_table(cqg_ctx *ctx, double **out) {
+  if (ctx->device < 0 || ctx->device >= kNoAllocMaxDevices) {
+    ctx->err = "cqg_one_e_noalloc: device ordinal out of range";
+    return CQG_ERR_BAD_ARG;
+  }
+  std::lock_guard<std::mutex> lock(g_oe_table_mutex);
+  if (!g_oe_table_addr[ctx->device]) {
+    void *p = nullptr;
+    CUCHK(cudaGetSymbolAddress(&p, g_oe_charge_table));
+    g_oe_table_addr[ctx->device] = (double *)p;
+  }
+  *out = g_oe_table_addr[ctx->device];
+  return CQG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+cqg_status cqg_one_e_noalloc(cqg_ctx *ctx, int ncharge, const double *Z, const double *R, double *S, double *T,
+                             double *V, int ld, void *stream) {
+  if (!ctx || ncharge < 0 || (ncharge > 0 && (!Z || !R)) || !S || !T || !V) return CQG_ERR_BAD_ARG;
+  if (ncharge > CQG_ONE_E_NOALLOC_MAX_CHARGES) {
+    ctx->err = "cqg_one_e_noalloc: ncharge exceeds CQG_ONE_E_NOALLOC_MAX_CHARGES (4096)";
+    return CQG_ERR_BAD_ARG;
+  }
+  if (ctx->nshell == 0) {
+    ctx->err = "cqg_set_basis has not been called";
+    return CQG_ERR_STATE;
+  }
+  if (ctx->nmol != 1) {
+    ctx->err = "cqg_one_e_noalloc is for single-molecule contexts";
+    return CQG_ERR_STATE;
+  }
+  if (ld < ctx->nbf) return CQG_ERR_BAD_ARG;
+  CUCHK(cudaSetDevice(ctx->device));
+  double *tab = nullptr;
+  const cqg_status s = oe_charge_table(ctx, &tab);
+  if (s != CQG_OK) return s;
+  cudaStream_t st = (cudaStream_t)stream;
+  // Z and R may be host or device pointers; the table is written in full for the
+  // `ncharge` entries the kernel reads, so nothing in it has to start at zero.
+  if (ncharge > 0) {
+    CUCHK(cudaMemcpyAsync(tab, Z, (size_t)ncharge * sizeof(double), cudaMemcpyDefault, st));
+    CUCHK(cudaMemcpyAsync(tab + ncharge, R, 3 * (size_t)ncharge * sizeof(double), cudaMemcpyDefault, st));
+  }
+  OneEShells sh;
+  sh.L = ctx->d_shL.p;
+  sh.nprim = ctx->d_shnp.p;
+  sh.poff = ctx->d_shpoff.p;
+  sh.bf = ctx->d_bf.p;
+  sh.alpha = ctx->d_alpha.p;
+  sh.coef = ctx->d_coef.p;
+  sh.center = ctx->d_center.p;
+  OneEMols om;
+  memset(&om, 0, sizeof(om));
+  const long long np = ctx->nallpairs;
+  k_one_e<<<(unsigned)((np + 63) / 64), 64, 0, st>>>(sh, ctx->d_allpairs.p, np, ncharge, tab,
+                                                     (const double3 *)(tab + ncharge), ctx->d_boys.p, S, T, V, ld,
+                                                     om);
+  CUCHK(cudaGetLastError());
+  return CQG_OK;
+}
+
+}  // extern "C"

@@ -120,6 +120,23 @@ cqg_status cqg_form_pt(cqg_ctx *ctx, int is_rhf, double xHF, const double *Ps,
 cqg_status cqg_one_e(cqg_ctx *ctx, int ncharge, const double *Z, const double *R, double *S,
                      double *T, double *V, int ld, int on_device, void *stream);
 
+/* cqg_one_e without any allocation: the same integrals and kernel as cqg_one_e with device
+ * S, T, V (leading dimension ld), but the point-charge table is held in a fixed
+ * module-scope device array of CQG_ONE_E_NOALLOC_MAX_CHARGES entries (4 doubles each,
+ * 128 KiB) instead of context scratch, so the call makes no cudaMalloc/cudaFree and calls
+ * no allocating library.  Z and R may be host or device pointers; work is enqueued on
+ * `stream`, nothing is synchronised.  ncharge > CQG_ONE_E_NOALLOC_MAX_CHARGES returns
+ * CQG_ERR_BAD_ARG (cqg_last_error says why).  Nothing has to start at zero: the table is
+ * written in full for the entries read and every element of S, T, V is written.
+ * The first call on a device resolves the array's device address (cudaGetSymbolAddress,
+ * with that device current); make that first call before any stream capture.  The array is
+ * shared by every context on a device: calls that overlap (other streams, threads or
+ * contexts on the same device) race on it and must be serialised by the caller.
+ * This entry point has no counterpart in the reference. */
+#define CQG_ONE_E_NOALLOC_MAX_CHARGES 4096
+cqg_status cqg_one_e_noalloc(cqg_ctx *ctx, int ncharge, const double *Z, const double *R,
+                             double *S, double *T, double *V, int ld, void *stream);
+
 /* ---- Batches: many independent molecules of uneven size in one context ----
  * cqg_set_basis_batch takes the shells of all molecules concatenated (molecule m has
  * nshell_per_mol[m] shells).  Matrices of a batch live on the device, packed: molecule m's
