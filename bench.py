@@ -239,6 +239,23 @@ def scf_compare(mol, bs, thresh, cutoff, sweep=()):
     t_plain, t_mixed = out["plain_fp64"]["seconds_to_1uEh"], out["mixed_incremental"]["seconds_to_1uEh"]
     if t_plain and t_mixed:
         out["speedup_time_to_1uEh"] = t_plain / t_mixed
+    # learned initial density (network trained on this engine's converged cluster densities)
+    from chronusq_public_b200.guess_model import PairMLP, default_weights
+    wpath = default_weights(bs.name)
+    if wpath:
+        net = PairMLP.load(wpath)
+        for key, mixed in (("learned_fp64", False), ("mixed_incremental_learned", True)):
+            lg = SingleSlater(mol, bs, ints=warm.ints)
+            lg.guess, lg.guess_model = "LEARNED", net
+            if mixed:
+                lg.precision, lg.fp32_cutoff, lg.incremental = "mixed", cutoff, True
+            E = lg.SCF3()
+            out[key] = {"energy": E, "abs_dE_vs_fp64": abs(E - E64), "iterations": lg.nSCFIter,
+                        "seconds": lg.scf_seconds, "seconds_to_1uEh": lg.time_to(E64, 1e-6),
+                        "guess_used": lg.guess_used, "weights": os.path.basename(wpath)}
+        t_learned = out["mixed_incremental_learned"]["seconds_to_1uEh"]
+        if t_plain and t_learned:
+            out["speedup_time_to_1uEh_mixed_learned"] = t_plain / t_learned
     warm.close()
     return out
 

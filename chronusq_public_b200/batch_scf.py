@@ -10,6 +10,7 @@ Fock matrix was built from, E = Tr(P h) + 1/4 Tr(P PT[P]) + E_nuc.
 """
 from __future__ import annotations
 
+import math
 import time
 from typing import List, Optional, Sequence
 
@@ -99,18 +100,57 @@ class BatchSCF:
                 view[b0:b0 + nb, b0:b0 + nb] = cache[z]
         return P
 
+    def learned_density(self, model):
+        """Packed densities predicted by `model` (guess_model.PairMLP, one forward pass for
+        all molecules), each projected on its natural orbitals (the nocc most occupied
+        eigenvectors of the orthonormal-basis density are occupied).  A molecule whose
+        prediction is not finite or whose Tr(PS) is more than 10 % off the electron count
+        takes the SAD superposition instead (projected the same way).  Returns the packed
+        density and the per-molecule flag of a usable prediction."""
+        from .guess_model import predict_densities
+        t = self.torch
+        P = self.B.zeros()
+        preds = predict_densities(model, self.mols, self.bss)
+        for m, Pm in enumerate(preds):
+            self.B.view(P, m).copy_(t.as_tensor(Pm, dtype=t.float64, device=self.dev))
+        ok = np.zeros(self.nmol, dtype=bool)
+        sad = None
+        for g in self.groups:
+            Pg = self.gather(P, g)
+            ne = (Pg * g["S"]).sum((-1, -2)).cpu().numpy()
+            nel = np.array([self.mols[m].nelectrons for m in g["members"]], dtype=float)
+            good = np.isfinite(ne) & (np.abs(ne - nel) <= 0.1 * nel)
+            ok[g["members"]] = good
+            if not good.all():
+                sad = self.sad_density() if sad is None else sad
+                keep = t.as_tensor(good, device=self.dev)[:, None, None]
+                Pg = t.where(keep, Pg, self.gather(sad, g))
+            Xi = g["S"] @ g["X"]                  # X^-1 = S^(1/2) for the Loewdin X
+            DO = Xi.transpose(-1, -2) @ Pg @ Xi
+            self.scatter(self._density(-DO, g), g, P)   # most occupied natural orbitals
+        return P, ok
+
     # ------------------------------------------------------------------ SCF ---
-    def run(self, density=None, use_graph: bool = False, autotune: bool = False):
+    def run(self, density=None, use_graph: bool = False, autotune: bool = False, model=None):
         """Converge every molecule; returns the per-molecule energies (numpy).
 
+        The guess density is the SAD superposition, or `density` (packed), or the one
+        `model` (guess_model.PairMLP) predicts, made inside the timed region.
         use_graph: the batched Fock build of every iteration is one CUDA-graph replay
         (captured once, after the guess build).  autotune: the guess build also picks the
         launch shape of every class work list."""
         t = self.torch
         t.cuda.synchronize(self.dev)
         t0 = time.perf_counter()
-        # guess: SAD superposition -> one batched Fock build -> diagonalise
-        P = self.sad_density() if density is None else density.clone()
+        # guess density -> one batched Fock build -> diagonalise; a learned guess is the
+        # first iterate itself, and its build is the first iteration's
+        first_PT = None
+        self.guess_fallbacks = 0
+        if model is not None:
+            P, ok = self.learned_density(model)
+            self.guess_fallbacks = int((~ok).sum())
+        else:
+            P = self.sad_density() if density is None else density.clone()
         if autotune:
             self.B.autotune_next()
         PT = self.B.formPT(P)
@@ -126,9 +166,12 @@ class BatchSCF:
                 P_static, PT_static = P.clone(), self.B.zeros()
                 graph = self.B.capture_formPT(P_static, PT_static)
                 self.graph_captures = 1
-        for g in self.groups:
-            F = 2.0 * g["H"] + self.gather(PT, g)
-            self.scatter(self._density(g["X"].transpose(-1, -2) @ F @ g["X"], g), g, P)
+        if model is not None:
+            first_PT = PT
+        else:
+            for g in self.groups:
+                F = 2.0 * g["H"] + self.gather(PT, g)
+                self.scatter(self._density(g["X"].transpose(-1, -2) @ F @ g["X"], g), g, P)
         active = np.ones(self.nmol, dtype=bool)
         Eold = t.zeros(self.nmol, dtype=t.float64, device=self.dev)
         energies = t.zeros(self.nmol, dtype=t.float64, device=self.dev)
@@ -140,7 +183,9 @@ class BatchSCF:
         self.fock_builds = 0
         self.log = []
         for it in range(self.maxSCFIter):
-            if graph is not None:
+            if first_PT is not None:
+                PT, first_PT = first_PT, None
+            elif graph is not None:
                 self.B.set_active(active.tolist())
                 P_static.copy_(P)
                 graph.replay()

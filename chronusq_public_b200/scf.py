@@ -26,7 +26,10 @@ Fock builds through :class:`~chronusq_public_b200.aointegrals.AOIntegrals`:
 * Guesses: SAD -- an atomic UHF per unique element (core guess, no DIIS), densities
   placed block-diagonally, spin-averaged, one molecular Fock build, diagonalised
   (singleslater_guess.h:100-264); CORE -- the core Hamiltonian diagonalised; or an
-  explicit density (the READ guess, guess.h:320-329).
+  explicit density (the READ guess, guess.h:320-329).  LEARNED (no reference
+  counterpart) starts the iterations from the density predicted by guess_model.PairMLP,
+  projected on its natural orbitals, falling back to SAD when the prediction is
+  unphysical; the converged energy does not depend on the guess.
 
 The per-iteration HDF5 traffic of the reference (writeSCFFiles, scfutils.h:1114-1188) has
 no counterpart: all state stays in device memory.
@@ -90,7 +93,9 @@ class SingleSlater:
         self.doDamp = True
         self.dampParam = 0.1
         self.xHF = -0.5
-        self.guess = "SAD"
+        self.guess = "SAD"             # "SAD", "CORE" or "LEARNED" (needs guess_model)
+        self.guess_model = None
+        self.guess_used = None
         # mixed precision + incremental (Delta D) Fock build
         self.precision = "fp64"        # "fp64" or "mixed"
         self.fp32_cutoff = 1e-8        # density-weighted Schwarz bound below which a quartet runs in FP32
@@ -191,6 +196,23 @@ class SingleSlater:
             Pz = (self.nOA - self.nOB) / (self.nOA + self.nOB) * Ps
         return Ps, Pz
 
+    def _learned_density(self):
+        """Density predicted by ``self.guess_model`` (a guess_model.PairMLP), projected on
+        its natural orbitals: the nOA (and nOB) eigenvectors of largest occupation of the
+        orthonormal-basis density are occupied, which gives the idempotent density with
+        the right electron counts nearest the prediction.  None when the prediction is not
+        finite or its Tr(PS) is more than 10 % off the electron count."""
+        from .guess_model import predict_density
+        t = self.torch
+        P = t.as_tensor(predict_density(self.guess_model, self.mol, self.basis), dtype=t.float64, device=self.dev)
+        ne = float(t.sum(P * self.overlap))
+        nel = self.mol.nelectrons
+        if not math.isfinite(ne) or abs(ne - nel) > 0.1 * nel:
+            return None
+        DO = self.X.T @ self.overlap @ P @ self.overlap @ self.X
+        DOs, DOz = self._diag_density(-DO, t.zeros_like(DO))
+        return self._unortho(DOs), self._unortho(DOz)
+
     def formGuess(self, density=None):
         """Returns (Ps, Pz, FOs, FOz): the starting density and the orthonormal Fock it
         came from (the damping reference of the first iteration)."""
@@ -203,6 +225,15 @@ class SingleSlater:
         elif self.guess == "CORE" or self.mol.natoms <= 1:
             return self._core_guess()
         elif self.guess == "SAD":
+            Ps, Pz = self._sad_density()
+            Fs, Fz, _, _ = self.formFock(Ps, Pz)
+        elif self.guess == "LEARNED":
+            # the projected prediction is the first iterate itself: no guess Fock build,
+            # and no damping reference for the first iteration
+            pred = self._learned_density()
+            self.guess_used = "SAD" if pred is None else "LEARNED"
+            if pred is not None:
+                return pred[0], pred[1], None, None
             Ps, Pz = self._sad_density()
             Fs, Fz, _, _ = self.formFock(Ps, Pz)
         else:
@@ -284,7 +315,7 @@ class SingleSlater:
                         FOs, FOz = self._ortho(Fs), self._ortho(Fz)
             if fp_converged:
                 diis_on = False
-            if damp > 0.0:
+            if damp > 0.0 and FOs_prev is not None:
                 FOs = (1.0 - damp) * FOs + damp * FOs_prev
                 if not self.isClosedShell:
                     FOz = (1.0 - damp) * FOz + damp * FOz_prev
