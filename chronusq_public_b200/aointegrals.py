@@ -118,6 +118,18 @@ class AOIntegrals:
     def setTiming(self, on: bool):
         _lib.check(self._L.cqg_set_timing(self._ctx, 1 if on else 0), self._ctx)
 
+    def autotune_next(self):
+        """The next contraction times every candidate launch shape of each quartet-class
+        work list and keeps the fastest for the later calls of this context."""
+        _lib.check(self._L.cqg_autotune_next(self._ctx), self._ctx)
+
+    def launch_shapes(self):
+        """(CTAs per SM, warps per CTA) chosen per class work list (0 = default)."""
+        cta = (ctypes.c_int * 110)()
+        wpb = (ctypes.c_int * 110)()
+        _lib.check(self._L.cqg_get_launch_shapes(self._ctx, cta, wpb), self._ctx)
+        return list(cta), list(wpb)
+
     # ------------------------------------------------------------------ queries ---
     def computeSchwartz(self) -> np.ndarray:
         ns = self.basisSet.nshell

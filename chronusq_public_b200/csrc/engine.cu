@@ -133,7 +133,7 @@ __device__ __forceinline__ void mol_view(const DigestGroups &dg, int g, int m, c
 template <int LA, int LB>
 __global__ void __launch_bounds__(128) k_schwarz(Pairs P, Shells S, const double *__restrict__ boys_g,
                                                  int beg, int end, double *__restrict__ Qout) {
-  __shared__ double boys[BOYS_NT * BOYS_SROW];
+  __shared__ __align__(16) double boys[BOYS_NT * BOYS_SROW];
   stage_boys<2 * (LA + LB)>(boys_g, boys);
   __syncthreads();
   int i = beg + blockIdx.x * blockDim.x + threadIdx.x;
@@ -499,11 +499,19 @@ __device__ __forceinline__ void eri_jk_one(const uint2 *__restrict__ ql, long lo
 // Per-thread class kernel: persistent grid over the class's quartet range; the Boys rows
 // of this class are staged in shared memory once per block.  T is the arithmetic type of
 // everything after the (FP64) Boys values; the digest accumulates in FP64.
+// Threads per block of the per-thread class kernels (each block stages its own copy of the
+// Boys rows in shared memory).  128 and 256 measure within 2 % of each other on (H2O)_32
+// cc-pVDZ; 512 caps registers at 128 and spills in the p/d classes.
+#ifndef CQG_ERI_THREADS
+#define CQG_ERI_THREADS 128
+#endif
+constexpr int kEriThreads = CQG_ERI_THREADS;
+
 template <int LA, int LB, int LC, int LD, typename T>
-__global__ void __launch_bounds__(128) k_eri_jk(const uint2 *__restrict__ ql, const long long *__restrict__ range,
+__global__ void __launch_bounds__(kEriThreads) k_eri_jk(const uint2 *__restrict__ ql, const long long *__restrict__ range,
                                                 int blk, Pairs P, Shells S, const double *__restrict__ boys_g,
                                                 DigestGroups dg) {
-  __shared__ double boys[BOYS_NT * BOYS_SROW];
+  __shared__ __align__(16) double boys[BOYS_NT * BOYS_SROW];
   stage_boys<LA + LB + LC + LD>(boys_g, boys);
   __syncthreads();
   const long long beg = range[2 * blk], end = range[2 * blk + 1];
@@ -1147,9 +1155,10 @@ static cudaError_t launch_eri(cqg_ctx *ctx, int blk, long long n, cudaStream_t s
   } else {
     const int cta = ctx->shape_cta[blk] > 0 ? ctx->shape_cta[blk] : 12;
     const long long cap = (long long)ctx->nsm * cta;
-    long long nb = n > 0 ? std::min<long long>((n + 127) / 128, cap) : cap;
-    k_eri_jk<LA, LB, LC, LD, T><<<(unsigned)nb, 128, 0, st>>>(ctx->d_qlist.p, ctx->d_range.p, blk, make_pairs(ctx),
-                                                           make_shells(ctx), ctx->d_boys.p, dg);
+    long long nb = n > 0 ? std::min<long long>((n + kEriThreads - 1) / kEriThreads, cap) : cap;
+    k_eri_jk<LA, LB, LC, LD, T><<<(unsigned)nb, kEriThreads, 0, st>>>(ctx->d_qlist.p, ctx->d_range.p, blk,
+                                                                   make_pairs(ctx), make_shells(ctx), ctx->d_boys.p,
+                                                                   dg);
     return cudaGetLastError();
   }
 }

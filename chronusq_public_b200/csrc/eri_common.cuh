@@ -53,28 +53,59 @@ __device__ __forceinline__ void boys_eval(double T, const double* __restrict__ t
   }
 }
 
-// Shared-memory copy of the rows a kernel of total angular momentum L needs:
-// s[i * BOYS_SROW + k] = F_{L+k}(0.1 i), k = 0..BOYS_NTAYLOR.
-#define BOYS_SROW (BOYS_NTAYLOR + 1)
+// Shared-memory copy of the rows a kernel of total angular momentum L needs, with the
+// Taylor coefficients already divided by k! and e^{-T_i} appended (16-byte aligned rows,
+// read as five double2):
+//   s[i * BOYS_SROW + k] = F_{L+k}(0.1 i) / k!,  k = 0..BOYS_NTAYLOR
+//   s[i * BOYS_SROW + BOYS_NTAYLOR + 1] = exp(-0.1 i)
+#define BOYS_SROW (BOYS_NTAYLOR + 2)
 template <int L>
 __device__ __forceinline__ void stage_boys(const double *__restrict__ tab, double *s) {
-  for (int k = threadIdx.x; k < BOYS_NT * BOYS_SROW; k += blockDim.x)
-    s[k] = __ldg(tab + (k / BOYS_SROW) * BOYS_NORD + L + (k % BOYS_SROW));
+  for (int k = threadIdx.x; k < BOYS_NT * BOYS_SROW; k += blockDim.x) {
+    const int i = k / BOYS_SROW, c = k % BOYS_SROW;
+    if (c <= BOYS_NTAYLOR) {
+      double inv_fact = 1.0;
+      for (int j = 2; j <= c; ++j) inv_fact /= (double)j;
+      s[k] = __ldg(tab + i * BOYS_NORD + L + c) * inv_fact;
+    } else {
+      s[k] = exp(-0.1 * (double)i);
+    }
+  }
 }
 
-// boys_eval with the table staged in shared memory (layout of stage_boys<L>)
+// boys_eval with the table staged in shared memory (layout of stage_boys<L>).  Below
+// BOYS_TMAX, e^{-T} = e^{-T_i} e^{x} with x = T_i - T, |x| <= 0.05, from the degree-9
+// Taylor polynomial of e^x (remainder < 3e-20 relative), instead of a call to exp().
 template <int L>
 __device__ __forceinline__ void boys_eval_sm(double T, const double *s, double *F) {
+  static_assert(BOYS_NTAYLOR == 8 && BOYS_SROW == 10, "row layout read as five double2");
   if (T < BOYS_TMAX) {
     const int i = __double2int_rn(T * 10.0);
     const double x = (double)i * 0.1 - T;
-    const double *row = s + i * BOYS_SROW;
-    double f = row[BOYS_NTAYLOR];
-#pragma unroll
-    for (int k = BOYS_NTAYLOR; k >= 1; --k) f = row[k - 1] + x * f * (1.0 / k);
+    const double2 *row = reinterpret_cast<const double2 *>(s + i * BOYS_SROW);
+    const double2 c01 = row[0], c23 = row[1], c45 = row[2], c67 = row[3], c8e = row[4];
+    double f = c8e.x;
+    f = fma(x, f, c67.y);
+    f = fma(x, f, c67.x);
+    f = fma(x, f, c45.y);
+    f = fma(x, f, c45.x);
+    f = fma(x, f, c23.y);
+    f = fma(x, f, c23.x);
+    f = fma(x, f, c01.y);
+    f = fma(x, f, c01.x);
     F[L] = f;
     if (L > 0) {
-      const double e = exp(-T);
+      double ex = 1.0 / 362880.0;
+      ex = fma(x, ex, 1.0 / 40320.0);
+      ex = fma(x, ex, 1.0 / 5040.0);
+      ex = fma(x, ex, 1.0 / 720.0);
+      ex = fma(x, ex, 1.0 / 120.0);
+      ex = fma(x, ex, 1.0 / 24.0);
+      ex = fma(x, ex, 1.0 / 6.0);
+      ex = fma(x, ex, 0.5);
+      ex = fma(x, ex, 1.0);
+      ex = fma(x, ex, 1.0);
+      const double e = c8e.y * ex;
       const double t2 = 2.0 * T;
 #pragma unroll
       for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * (1.0 / (2 * m + 1));
