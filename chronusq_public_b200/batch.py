@@ -125,11 +125,14 @@ class BatchAOIntegrals:
         _lib.check(self._L.cqg_get_launch_shapes(self._ctx, cta.ctypes.data_as(i), wpb.ctypes.data_as(i)), self._ctx)
         return cta, wpb
 
-    def capture_formPT(self, P_static, PT_static, xHF: float = -0.5):
+    def capture_formPT(self, P_static, PT_static, xHF: float = -0.5, warm: bool = True):
         """CUDA graph of one batched RHF Fock build reading P_static, writing PT_static.
-        Graph mode must be on; the call is run once uncaptured first (kernel attributes)."""
+        Graph mode must be on.  With `warm`, the call is first run once uncaptured, which
+        sets the kernels' attributes; a context that has already run a contraction of the
+        same molecules can skip it."""
         torch = self.torch
-        self.formPT(P_static, xHF=xHF, PTs=PT_static)
+        if warm:
+            self.formPT(P_static, xHF=xHF, PTs=PT_static)
         torch.cuda.synchronize(self.device)
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):

@@ -158,14 +158,12 @@ class BatchSCF:
         self.graph_replays = 0
         self.graph_captures = 0
         if use_graph:
+            # the graph is captured after the first iteration's build, which is run
+            # uncaptured: its screened count sizes the list capacity (the guess build's
+            # count, from a block-diagonal density, is far smaller)
             free, _ = t.cuda.mem_get_info(self.dev)
             self.graph_memory_limit = 0.4 * free
-            cap = 2 * self.B.stats()["quartets"] + 4096
-            if cap * 8 <= self.graph_memory_limit:
-                self.B.enable_graph(cap, 1)
-                P_static, PT_static = P.clone(), self.B.zeros()
-                graph = self.B.capture_formPT(P_static, PT_static)
-                self.graph_captures = 1
+            P_static, PT_static = None, self.B.zeros()
         if model is not None:
             first_PT = PT
         else:
@@ -181,17 +179,22 @@ class BatchSCF:
             g["FO_prev"] = None
         self.iterations = np.zeros(self.nmol, dtype=int)
         self.fock_builds = 0
+        self.fock_seconds = 0.0           # wall time of the Fock builds (device-synchronised)
         self.log = []
         for it in range(self.maxSCFIter):
+            t.cuda.synchronize(self.dev)
+            tf = time.perf_counter()
             if first_PT is not None:
                 PT, first_PT = first_PT, None
+            elif use_graph and it == 0:
+                PT = self.B.formPT(P, active=active.tolist())
             elif graph is not None:
                 self.B.set_active(active.tolist())
                 P_static.copy_(P)
                 graph.replay()
                 st = self.B.graph_status()
                 if st["overflow"]:
-                    # the list capacity was sized on the guess build: rebuild this iteration
+                    # more quartets than the capture's list capacity: rebuild this iteration
                     # without the graph, then recapture with room for this density's quartets
                     self.B.enable_graph(0)
                     self.B.set_active(None)
@@ -202,7 +205,7 @@ class BatchSCF:
                         self.B.set_active(None)
                         self.B.enable_graph(need, 1)
                         P_static.copy_(P)
-                        graph = self.B.capture_formPT(P_static, PT_static)
+                        graph = self.B.capture_formPT(P_static, PT_static, warm=False)
                         self.graph_captures += 1
                 else:
                     PT = PT_static
@@ -210,6 +213,16 @@ class BatchSCF:
             else:
                 PT = self.B.formPT(P, active=active.tolist())
             self.fock_builds += 1
+            t.cuda.synchronize(self.dev)
+            self.fock_seconds += time.perf_counter() - tf
+            if use_graph and graph is None and P_static is None:
+                need = int(1.25 * self.B.stats()["quartets"]) + 4096
+                P_static = P.clone()
+                if need * 8 <= self.graph_memory_limit:
+                    self.B.set_active(None)
+                    self.B.enable_graph(need, 1)
+                    graph = self.B.capture_formPT(P_static, PT_static, warm=False)
+                    self.graph_captures = 1
             Pnew = P.clone()
             for g in self.groups:
                 gidx = g["idx"]

@@ -1568,15 +1568,26 @@ static cqg_status autotune_shapes(cqg_ctx *ctx, const long long *crange, cudaStr
     } else {
       for (int c : {4, 8, 12, 16, 24}) cand.push_back({c, 0});
     }
+    // Long lists are timed on their first quarter (at least 2^20 quartets), after one
+    // untimed run, one run per candidate; short lists in full, best of two runs.  The
+    // kernels read their range from d_range, so the sample range is written there and the
+    // full range put back afterwards.
+    const long long m = n > (1ll << 20) ? std::max<long long>(1ll << 20, n / 4) : n;
+    const int reps = m < n ? 1 : 2;
+    if (m < n) {
+      const long long sub[2] = {crange[2 * vb], crange[2 * vb] + m};
+      CUCHK(cudaMemcpyAsync(ctx->d_range.p + 2 * vb, sub, sizeof(sub), cudaMemcpyHostToDevice, st));
+    }
     float best = 1e30f;
     std::pair<int, int> pick = cand[0];
-    for (auto &cw : cand) {
+    for (int ci = (m < n ? -1 : 0); ci < (int)cand.size(); ++ci) {
+      const std::pair<int, int> cw = cand[ci < 0 ? 0 : ci];
       ctx->shape_cta[vb] = cw.first;
       ctx->shape_wpb[vb] = cw.second;
       float tbest = 1e30f;
-      for (int rep = 0; rep < 2; ++rep) {
+      for (int rep = 0; rep < (ci < 0 ? 1 : reps); ++rep) {
         cudaEventRecord(e0, st);
-        cudaError_t e = (vb < CQG_NQC ? kEriLaunch[k] : kEriLaunch32[k])(ctx, vb, n, st, scratch);
+        cudaError_t e = (vb < CQG_NQC ? kEriLaunch[k] : kEriLaunch32[k])(ctx, vb, m, st, scratch);
         cudaEventRecord(e1, st);
         if (e != cudaSuccess) {
           cudaEventDestroy(e0);
@@ -1589,11 +1600,13 @@ static cqg_status autotune_shapes(cqg_ctx *ctx, const long long *crange, cudaStr
         cudaEventElapsedTime(&ms, e0, e1);
         tbest = std::min(tbest, ms);
       }
-      if (tbest < best) {
+      if (ci >= 0 && tbest < best) {
         best = tbest;
         pick = cw;
       }
     }
+    if (m < n) CUCHK(cudaMemcpyAsync(ctx->d_range.p + 2 * vb, crange + 2 * vb, 2 * sizeof(long long),
+                                     cudaMemcpyHostToDevice, st));
     ctx->shape_cta[vb] = pick.first;
     ctx->shape_wpb[vb] = pick.second;
   }

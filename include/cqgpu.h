@@ -42,8 +42,9 @@ enum { CQG_COULOMB = 0, CQG_EXCHANGE = 1 };
 /* precision policy of the quartet evaluation */
 enum {
   CQG_PREC_FP64 = 0,         /* every quartet in FP64 (the reference's arithmetic) */
-  CQG_PREC_MIXED = 1         /* quartets whose Schwarz product Q_ab*Q_cd is below the
-                                FP32 cutoff are evaluated in FP32, accumulated in FP64 */
+  CQG_PREC_MIXED = 1         /* quartets whose density-weighted Schwarz bound (the screen's
+                                max block norm * Q_ab * Q_cd) is below the FP32 cutoff are
+                                evaluated in FP32, accumulated in FP64 */
 };
 
 typedef struct cqg_ctx cqg_ctx;
@@ -86,7 +87,8 @@ cqg_status cqg_set_basis(cqg_ctx *ctx, int nshell, const int *L, const int *pure
 /* AOIntegrals::thresholdSchwartz_ (include/aointegrals.h:334; default 1e-14). */
 cqg_status cqg_set_threshold(cqg_ctx *ctx, double thresh);
 
-/* Precision policy; `fp32_cutoff` is the Schwarz-product cutoff for CQG_PREC_MIXED. */
+/* Precision policy; `fp32_cutoff` is the density-weighted bound below which a quartet runs
+ * in FP32 under CQG_PREC_MIXED. */
 cqg_status cqg_set_precision(cqg_ctx *ctx, int policy, double fp32_cutoff);
 
 /* Copy the nshell x nshell Schwarz matrix (column-major) to host memory. */
