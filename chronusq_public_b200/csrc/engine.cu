@@ -22,6 +22,7 @@
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/cqgpu.h"
@@ -557,6 +558,28 @@ __device__ __forceinline__ void eri_jk_one(const uint2 *__restrict__ ql, long lo
 // ------------------------------------------------------------- warp-mode classes ---
 // SCHWARZ = false: quartets from the list, J/K digest.  SCHWARZ = true: "quartet" i is
 // pair i with itself, and the kernel writes Q(i) = sqrt(max |(ab|ab)| diagonal).
+// One FP64 tensor-core step D += A B on an 8x8x4 tile (mma.sync m8n8k4 .f64).  Fragments:
+// a = A[g][t], b = B[t][g], d[i] = D[g][2t+i] with g = lane / 4, t = lane % 4.
+__device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+// Whether a warp class runs its two Hermite contractions on the FP64 tensor cores:
+//   W[h][cd] += sum_k R[h + k] KC[k][cd]     (per primitive quartet; KC = signed ket E products)
+//   C[ab][cd] += sum_h EB[ab][h] W[h][cd]    (per bra primitive pair)
+// W's 8x8 tiles are held in registers across the ket loop, so classes with more than 25
+// tiles keep the shared-memory loops.  FP32 lists keep them too (m8n8k4 is FP64 only).
+template <int LA, int LB, int LC, int LD, bool SCHWARZ, typename T>
+struct WarpMma {
+  static constexpr int HP = warpmd::nherm(LA + LB), HQ = warpmd::nherm(LC + LD);
+  static constexpr int NCCD = warpmd::ncart(LC) * warpmd::ncart(LD), NCAB = warpmd::ncart(LA) * warpmd::ncart(LB);
+  static constexpr int MT = (HP + 7) / 8, NT = (NCCD + 7) / 8, KT = (HQ + 3) / 4;
+  static constexpr int MTC = (NCAB + 7) / 8, KTH = (HP + 3) / 4;
+  static constexpr bool on = std::is_same<T, double>::value && !SCHWARZ && MT * NT <= 25;
+};
+
 template <int LA, int LB, int LC, int LD, bool SCHWARZ, typename T>
 __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ ql, const long long *__restrict__ range,
                                                      int blk, long long sbeg, long long send, Pairs P, Shells S,
@@ -571,6 +594,17 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
   __shared__ int s_h[WD::HL];
   __shared__ int s_cab[WD::NCAB];
   __shared__ int s_ccd[NCCD];
+  using MM = WarpMma<LA, LB, LC, LD, SCHWARZ, T>;
+  // s_sum[h * HQ + k]: index of the Hermite triple h + k (bra h, ket k) in R
+  __shared__ short s_sum[MM::on ? MM::HP * MM::HQ : 1];
+  if constexpr (MM::on) {
+    for (int k = threadIdx.x; k < MM::HP * MM::HQ; k += blockDim.x) {
+      int t1, u1, v1, t2, u2, v2;
+      warpmd::herm_of(k / MM::HQ, t1, u1, v1);
+      warpmd::herm_of(k % MM::HQ, t2, u2, v2);
+      s_sum[k] = (short)warpmd::hidx(t1 + t2, u1 + u2, v1 + v2);
+    }
+  }
   for (int k = threadIdx.x; k < WD::HL; k += blockDim.x) {
     int t, u, v;
     warpmd::herm_of(k, t, u, v);
@@ -629,7 +663,15 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
         const double Bc = lane == 0 ? B.x : (lane == 1 ? B.y : B.z);
         warpmd::build_E1<LA, LB, T>(Eb + lane * WD::NEB, T(Pc - Ac), T(Pc - Bc), T(0.5 * bp.ip));
       }
-      for (int k = lane; k < WD::NW; k += 32) W[k] = T(0);
+      double wacc[MM::on ? MM::MT : 1][MM::on ? MM::NT : 1][2];
+      if constexpr (MM::on) {
+#pragma unroll
+        for (int mt = 0; mt < MM::MT; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < MM::NT; ++nt) wacc[mt][nt][0] = wacc[mt][nt][1] = 0.0;
+      } else {
+        for (int k = lane; k < WD::NW; k += 32) W[k] = T(0);
+      }
       for (int ik = 0; ik < nk; ++ik) {
         const PrimPair kp = pkp[ik];
         __syncwarp();
@@ -691,6 +733,41 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
         }
         __syncwarp();
         const T *R = cur;  // level 0
+        if constexpr (MM::on) {
+          // A[h][k] = R[h + k] gathered from shared memory, B[k][cd] = signed ket E product
+          const int g = lane >> 2, tq = lane & 3;
+          constexpr int NTQ = WD::Q + 1;
+#pragma unroll
+          for (int kt = 0; kt < MM::KT; ++kt) {
+            const int k = kt * 4 + tq;
+            double a[MM::MT];
+#pragma unroll
+            for (int mt = 0; mt < MM::MT; ++mt) {
+              const int h = mt * 8 + g;
+              a[mt] = (h < MM::HP && k < MM::HQ) ? (double)R[s_sum[h * MM::HQ + k]] : 0.0;
+            }
+            const int kc = k < MM::HQ ? s_h[k] : 0;
+            const int kx = kc & 15, ky = (kc >> 4) & 15, kz = kc >> 8;
+#pragma unroll
+            for (int nt = 0; nt < MM::NT; ++nt) {
+              const int c = nt * 8 + g;
+              double b = 0.0;
+              if (k < MM::HQ && c < NCCD) {
+                const int cc = s_ccd[c];
+                const int cx = cc & 15, cy = (cc >> 4) & 15, cz = (cc >> 8) & 15;
+                const int dx = (cc >> 12) & 15, dy = (cc >> 16) & 15, dz = cc >> 20;
+                if (kx <= cx + dx && ky <= cy + dy && kz <= cz + dz) {
+                  b = (double)Ek[(cx * (LD + 1) + dx) * NTQ + kx] *
+                      (double)Ek[WD::NEK + (cy * (LD + 1) + dy) * NTQ + ky] *
+                      (double)Ek[2 * WD::NEK + (cz * (LD + 1) + dz) * NTQ + kz];
+                  if ((kx + ky + kz) & 1) b = -b;
+                }
+              }
+#pragma unroll
+              for (int mt = 0; mt < MM::MT; ++mt) dmma_884(wacc[mt][nt], a[mt], b);
+            }
+          }
+        } else
         // W[tuv][cd] += sum (-1)^(tau+nu+phi) E^cd R
         for (int e2 = lane; e2 < WD::NW; e2 += 32) {
           const int h = e2 / NCCD, c = e2 % NCCD;
@@ -715,6 +792,56 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
         }
       }
       __syncwarp();
+      if constexpr (MM::on) {
+        const int g = lane >> 2, tq = lane & 3;
+        constexpr int NTP = WD::P + 1;
+        // W tiles to shared memory, then C[ab][cd] += EB[ab][h] W[h][cd] on the tensor cores
+#pragma unroll
+        for (int mt = 0; mt < MM::MT; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < MM::NT; ++nt)
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+              const int h = mt * 8 + g, c = nt * 8 + tq * 2 + i;
+              if (h < MM::HP && c < NCCD) W[h * NCCD + c] = wacc[mt][nt][i];
+            }
+        __syncwarp();
+        for (int mtc = 0; mtc < MM::MTC; ++mtc) {
+          const int abi = mtc * 8 + g;
+          const int cab = abi < MM::NCAB ? s_cab[abi] : 0;
+          const int ax = cab & 15, ay = (cab >> 4) & 15, az = (cab >> 8) & 15;
+          const int bx = (cab >> 12) & 15, by = (cab >> 16) & 15, bz = cab >> 20;
+          for (int nt = 0; nt < MM::NT; ++nt) {
+            double cf[2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+              const int c = nt * 8 + tq * 2 + i;
+              cf[i] = (abi < MM::NCAB && c < NCCD) ? (double)Cc[abi * NCCD + c] : 0.0;
+            }
+#pragma unroll
+            for (int kt = 0; kt < MM::KTH; ++kt) {
+              const int h = kt * 4 + tq;
+              double a = 0.0;
+              if (abi < MM::NCAB && h < MM::HP) {
+                const int hc = s_h[h];
+                const int t = hc & 15, u = (hc >> 4) & 15, v = hc >> 8;
+                if (t <= ax + bx && u <= ay + by && v <= az + bz)
+                  a = (double)Eb[(ax * (LB + 1) + bx) * NTP + t] *
+                      (double)Eb[WD::NEB + (ay * (LB + 1) + by) * NTP + u] *
+                      (double)Eb[2 * WD::NEB + (az * (LB + 1) + bz) * NTP + v];
+              }
+              const int hb = kt * 4 + tq, cb = nt * 8 + g;
+              const double b = (hb < MM::HP && cb < NCCD) ? (double)W[hb * NCCD + cb] : 0.0;
+              dmma_884(cf, a, b);
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+              const int c = nt * 8 + tq * 2 + i;
+              if (abi < MM::NCAB && c < NCCD) Cc[abi * NCCD + c] = (T)cf[i];
+            }
+          }
+        }
+      } else
       // C[ab][cd] += sum_tuv E^ab_tuv W[tuv][cd]
       for (int e2 = lane; e2 < WD::NC; e2 += 32) {
         const int abi = e2 / NCCD, c = e2 % NCCD;
