@@ -570,14 +570,15 @@ __device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
 //   W[h][cd] += sum_k R[h + k] KC[k][cd]     (per primitive quartet; KC = signed ket E products)
 //   C[ab][cd] += sum_h EB[ab][h] W[h][cd]    (per bra primitive pair)
 // W's 8x8 tiles are held in registers across the ket loop, so classes with more than 25
-// tiles keep the shared-memory loops.  FP32 lists keep them too (m8n8k4 is FP64 only).
+// tiles keep the shared-memory loops.  FP32 lists use the same FP64 tiles: their R and E
+// values are FP32 and the products are accumulated in FP64.
 template <int LA, int LB, int LC, int LD, bool SCHWARZ, typename T>
 struct WarpMma {
   static constexpr int HP = warpmd::nherm(LA + LB), HQ = warpmd::nherm(LC + LD);
   static constexpr int NCCD = warpmd::ncart(LC) * warpmd::ncart(LD), NCAB = warpmd::ncart(LA) * warpmd::ncart(LB);
   static constexpr int MT = (HP + 7) / 8, NT = (NCCD + 7) / 8, KT = (HQ + 3) / 4;
   static constexpr int MTC = (NCAB + 7) / 8, KTH = (HP + 3) / 4;
-  static constexpr bool on = std::is_same<T, double>::value && !SCHWARZ && MT * NT <= 25;
+  static constexpr bool on = !SCHWARZ && MT * NT <= 25;
 };
 
 template <int LA, int LB, int LC, int LD, bool SCHWARZ, typename T>
