@@ -579,6 +579,10 @@ struct WarpMma {
   static constexpr int MT = (HP + 7) / 8, NT = (NCCD + 7) / 8, KT = (HQ + 3) / 4;
   static constexpr int MTC = (NCAB + 7) / 8, KTH = (HP + 3) / 4;
   static constexpr bool on = !SCHWARZ && MT * NT <= 25;
+  // larger classes accumulate W in shared memory, NTB column tiles at a time
+  static constexpr bool onS = !SCHWARZ && !on;
+  static constexpr int NTB = MT >= 25 ? 1 : 25 / MT;
+  static constexpr bool any = on || onS;
 };
 
 template <int LA, int LB, int LC, int LD, bool SCHWARZ, typename T>
@@ -597,8 +601,8 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
   __shared__ int s_ccd[NCCD];
   using MM = WarpMma<LA, LB, LC, LD, SCHWARZ, T>;
   // s_sum[h * HQ + k]: index of the Hermite triple h + k (bra h, ket k) in R
-  __shared__ short s_sum[MM::on ? MM::HP * MM::HQ : 1];
-  if constexpr (MM::on) {
+  __shared__ short s_sum[MM::any ? MM::HP * MM::HQ : 1];
+  if constexpr (MM::any) {
     for (int k = threadIdx.x; k < MM::HP * MM::HQ; k += blockDim.x) {
       int t1, u1, v1, t2, u2, v2;
       warpmd::herm_of(k / MM::HQ, t1, u1, v1);
@@ -768,6 +772,62 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
               for (int mt = 0; mt < MM::MT; ++mt) dmma_884(wacc[mt][nt], a[mt], b);
             }
           }
+        } else if constexpr (MM::onS) {
+          // the same product, with W read from and written back to shared memory for each
+          // block of NTB column tiles (every element is owned by one lane throughout)
+          const int g = lane >> 2, tq = lane & 3;
+          constexpr int NTQ = WD::Q + 1;
+          for (int n0 = 0; n0 < MM::NT; n0 += MM::NTB) {
+            double wb[MM::MT][MM::NTB][2];
+#pragma unroll
+            for (int mt = 0; mt < MM::MT; ++mt)
+#pragma unroll
+              for (int j = 0; j < MM::NTB; ++j)
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                  const int h = mt * 8 + g, c = (n0 + j) * 8 + tq * 2 + i;
+                  wb[mt][j][i] = (n0 + j < MM::NT && h < MM::HP && c < NCCD) ? (double)W[h * NCCD + c] : 0.0;
+                }
+#pragma unroll 1
+            for (int kt = 0; kt < MM::KT; ++kt) {
+              const int k = kt * 4 + tq;
+              double a[MM::MT];
+#pragma unroll
+              for (int mt = 0; mt < MM::MT; ++mt) {
+                const int h = mt * 8 + g;
+                a[mt] = (h < MM::HP && k < MM::HQ) ? (double)R[s_sum[h * MM::HQ + k]] : 0.0;
+              }
+              const int kc = k < MM::HQ ? s_h[k] : 0;
+              const int kx = kc & 15, ky = (kc >> 4) & 15, kz = kc >> 8;
+#pragma unroll
+              for (int j = 0; j < MM::NTB; ++j) {
+                const int c = (n0 + j) * 8 + g;
+                double b = 0.0;
+                if (k < MM::HQ && n0 + j < MM::NT && c < NCCD) {
+                  const int cc = s_ccd[c];
+                  const int cx = cc & 15, cy = (cc >> 4) & 15, cz = (cc >> 8) & 15;
+                  const int dx = (cc >> 12) & 15, dy = (cc >> 16) & 15, dz = cc >> 20;
+                  if (kx <= cx + dx && ky <= cy + dy && kz <= cz + dz) {
+                    b = (double)Ek[(cx * (LD + 1) + dx) * NTQ + kx] *
+                        (double)Ek[WD::NEK + (cy * (LD + 1) + dy) * NTQ + ky] *
+                        (double)Ek[2 * WD::NEK + (cz * (LD + 1) + dz) * NTQ + kz];
+                    if ((kx + ky + kz) & 1) b = -b;
+                  }
+                }
+#pragma unroll
+                for (int mt = 0; mt < MM::MT; ++mt) dmma_884(wb[mt][j], a[mt], b);
+              }
+            }
+#pragma unroll
+            for (int mt = 0; mt < MM::MT; ++mt)
+#pragma unroll
+              for (int j = 0; j < MM::NTB; ++j)
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                  const int h = mt * 8 + g, c = (n0 + j) * 8 + tq * 2 + i;
+                  if (n0 + j < MM::NT && h < MM::HP && c < NCCD) W[h * NCCD + c] = (T)wb[mt][j][i];
+                }
+          }
         } else
         // W[tuv][cd] += sum (-1)^(tau+nu+phi) E^cd R
         for (int e2 = lane; e2 < WD::NW; e2 += 32) {
@@ -793,19 +853,21 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
         }
       }
       __syncwarp();
-      if constexpr (MM::on) {
+      if constexpr (MM::any) {
         const int g = lane >> 2, tq = lane & 3;
         constexpr int NTP = WD::P + 1;
         // W tiles to shared memory, then C[ab][cd] += EB[ab][h] W[h][cd] on the tensor cores
+        if constexpr (MM::on) {
 #pragma unroll
-        for (int mt = 0; mt < MM::MT; ++mt)
+          for (int mt = 0; mt < MM::MT; ++mt)
 #pragma unroll
-          for (int nt = 0; nt < MM::NT; ++nt)
+            for (int nt = 0; nt < MM::NT; ++nt)
 #pragma unroll
-            for (int i = 0; i < 2; ++i) {
-              const int h = mt * 8 + g, c = nt * 8 + tq * 2 + i;
-              if (h < MM::HP && c < NCCD) W[h * NCCD + c] = wacc[mt][nt][i];
-            }
+              for (int i = 0; i < 2; ++i) {
+                const int h = mt * 8 + g, c = nt * 8 + tq * 2 + i;
+                if (h < MM::HP && c < NCCD) W[h * NCCD + c] = wacc[mt][nt][i];
+              }
+        }
         __syncwarp();
         for (int mtc = 0; mtc < MM::MTC; ++mtc) {
           const int abi = mtc * 8 + g;
