@@ -157,7 +157,7 @@ struct XList {
   int n;
 };
 __global__ void k_blocknorm(XList xl, int ldx, Mols mols, const int *__restrict__ bf,
-                            const int *__restrict__ sz, double *__restrict__ M,
+                            const int *__restrict__ sz, double *__restrict__ M, double *__restrict__ MT,
                             int *__restrict__ flags, double sym_tol) {
   const int mol = blockIdx.z;
   const int nsh = mols.nsh[mol];
@@ -165,8 +165,10 @@ __global__ void k_blocknorm(XList xl, int ldx, Mols mols, const int *__restrict_
   int s2 = blockIdx.y;
   if (s1 >= nsh || s2 >= nsh) return;
   double *Mm = M + mols.Moff[mol];
+  double *MTm = MT + mols.Moff[mol];
   if (!mols.active[mol]) {
     Mm[(size_t)s1 + (size_t)s2 * nsh] = 0.0;
+    MTm[(size_t)s2 + (size_t)s1 * nsh] = 0.0;
     return;
   }
   const int g1 = mols.shoff[mol] + s1, g2 = mols.shoff[mol] + s2;
@@ -188,6 +190,7 @@ __global__ void k_blocknorm(XList xl, int ldx, Mols mols, const int *__restrict_
       }
   }
   Mm[(size_t)s1 + (size_t)s2 * nsh] = mx;
+  MTm[(size_t)s2 + (size_t)s1 * nsh] = mx;   // transposed copy: M(s1, .) as a contiguous column
   if (bad) atomicOr(flags + 0, 1);
   if (asym) atomicOr(flags + 1, 1);
 }
@@ -239,16 +242,19 @@ __device__ __forceinline__ int coarse_range(const double *__restrict__ Q, int kb
 }
 
 // Density-weighted Schwarz bound of a quartet: max of the six shell-block norms of the
-// density times Q_ab Q_cd (contract.h:112-131).
-__device__ __forceinline__ double quartet_bound(const double *__restrict__ M, int nsh, int shoff, int2 ab, int2 cd,
-                                                double qab, double qcd) {
-  const int s1 = ab.x - shoff, s2 = ab.y - shoff, s3 = cd.x - shoff, s4 = cd.y - shoff;
-  double m = M[s1 + (size_t)s4 * nsh];
-  m = fmax(m, M[s2 + (size_t)s4 * nsh]);
+// density times Q_ab Q_cd (contract.h:112-131).  The four norms that pair a bra shell with
+// a ket shell are read from the transposed copy MT, where M(s1, .) and M(s2, .) are the
+// contiguous columns s1 and s2 (one pair of columns per bra pair, so they stay in L1);
+// m12 = M(s1, s2) is the bra's own, the same for every ket.
+__device__ __forceinline__ double quartet_bound(const double *__restrict__ M, const double *__restrict__ col1,
+                                                const double *__restrict__ col2, double m12, int nsh, int shoff,
+                                                int2 cd, double qab, double qcd) {
+  const int s3 = cd.x - shoff, s4 = cd.y - shoff;
+  double m = fmax(m12, col1[s4]);
+  m = fmax(m, col2[s4]);
   m = fmax(m, M[s3 + (size_t)s4 * nsh]);
-  m = fmax(m, M[s1 + (size_t)s3 * nsh]);
-  m = fmax(m, M[s2 + (size_t)s3 * nsh]);
-  m = fmax(m, M[s1 + (size_t)s2 * nsh]);
+  m = fmax(m, col1[s3]);
+  m = fmax(m, col2[s3]);
   return m * qab * qcd;
 }
 
@@ -258,7 +264,7 @@ __device__ __forceinline__ double quartet_bound(const double *__restrict__ M, in
 // (counts cnt[ntask + task], offsets off[ntask + task]); the rest to the FP64 list.
 template <bool FILL>
 __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pairs P, const double *__restrict__ M,
-                                                  Mols mols, const int *__restrict__ shmol,
+                                                  const double *__restrict__ MT, Mols mols, const int *__restrict__ shmol,
                                                   const double *__restrict__ Mmax, double thresh,
                                                   double cut32, long long *__restrict__ cnt,
                                                   const long long *__restrict__ off, uint2 *__restrict__ qlist,
@@ -280,6 +286,9 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
   const int mol = shmol[ab.x];
   const int nsh = mols.nsh[mol], shoff = mols.shoff[mol];
   const double *Mm = M + mols.Moff[mol];
+  const double *col1 = MT + mols.Moff[mol] + (size_t)(ab.x - shoff) * nsh;
+  const double *col2 = MT + mols.Moff[mol] + (size_t)(ab.y - shoff) * nsh;
+  const double m12 = Mm[(ab.x - shoff) + (size_t)(ab.y - shoff) * nsh];
   const int *bkt = mols.molbk + ((size_t)mol * CQG_NPC + bt.ket_class[blk]) * (CQG_NBUCKET + 1);
   const long long base64 = FILL ? off[warp] - obase : 0, base32 = FILL ? off[ntask + warp] - obase : 0;
   long long c64 = 0, c32 = 0;
@@ -294,7 +303,7 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
         int ket = k0 + lane;
         bool pass = false, lo = false;
         if (ket < kend) {
-          const double bnd = quartet_bound(Mm, nsh, shoff, ab, P.sh[ket], qb, P.Q[ket]);
+          const double bnd = quartet_bound(Mm, col1, col2, m12, nsh, shoff, P.sh[ket], qb, P.Q[ket]);
           pass = bnd >= thresh;
           lo = pass && bnd < cut32;
         }
@@ -1713,7 +1722,7 @@ cqg_status cqg_set_basis_batch(cqg_ctx *ctx, int nmol, const int *nshell_per_mol
   size_t scan_bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (long long *)nullptr, (long long *)nullptr, std::max(2 * task, 1));
   if (ctx->d_cnt.reserve(2 * task + 1) || ctx->d_off.reserve(2 * task + 1) || ctx->d_range.reserve(4 * CQG_NQC) ||
-      ctx->d_scan_tmp.reserve(scan_bytes + 16) || ctx->d_M.reserve((size_t)std::max(ctx->Mtotal, 1LL)) ||
+      ctx->d_scan_tmp.reserve(scan_bytes + 16) || ctx->d_M.reserve(2 * (size_t)std::max(ctx->Mtotal, 1LL)) ||
       ctx->d_Mmax.reserve(1) || ctx->d_flags.reserve(4) || ctx->d_blkacc.reserve(4 * CQG_NQC))
     return CQG_ERR_OOM;
   return CQG_OK;
@@ -1828,20 +1837,20 @@ static cqg_status contract_graph(cqg_ctx *ctx, int ngroups, const double *const 
   CUCHK(cudaMemsetAsync(ctx->d_G.p, 0, (size_t)ngroups * gsize * sizeof(double), st));
   {
     dim3 g((ctx->max_nsh + 127) / 128, ctx->max_nsh, ctx->nmol);
-    k_blocknorm<<<g, 128, 0, st>>>(xl, ldx, mols, ctx->d_bf.p, ctx->d_sz.p, ctx->d_M.p, ctx->d_flags.p, 1e-12);
+    k_blocknorm<<<g, 128, 0, st>>>(xl, ldx, mols, ctx->d_bf.p, ctx->d_sz.p, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, ctx->d_flags.p, 1e-12);
     const long long nn = ctx->Mtotal;
     k_maxreduce<<<(int)std::min<long long>((nn + 255) / 256, 1184), 256, 0, st>>>(ctx->d_M.p, nn, ctx->d_Mmax.p);
   }
   Pairs P = make_pairs(ctx);
   const int nb = (ctx->ntask + 7) / 8;
-  k_quartets<false><<<nb, 256, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
+  k_quartets<false><<<nb, 256, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
                                          ctx->thresh, cut32, ctx->d_cnt.p, nullptr, nullptr, ctx->d_blkacc.p, 0, 0, 0,
                                          0);
   size_t scan_bytes = ctx->d_scan_tmp.n;
   CUCHK(cub::DeviceScan::ExclusiveSum(ctx->d_scan_tmp.p, scan_bytes, ctx->d_cnt.p, ctx->d_off.p, 2 * ctx->ntask, st));
   k_block_ranges<<<1, 128, 0, st>>>(ctx->bt, ctx->ntask, ctx->d_cnt.p, ctx->d_off.p, ctx->d_range.p,
                                     ctx->graph_capacity, ctx->d_flags.p);
-  k_quartets<true><<<nb, 256, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
+  k_quartets<true><<<nb, 256, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
                                         ctx->thresh, cut32, nullptr, ctx->d_off.p, ctx->d_qlist.p, nullptr, 0,
                                         2LL * ctx->ntask, 0, ctx->graph_capacity);
   CUCHK(cudaGetLastError());
@@ -1902,7 +1911,7 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
   ctx->launches = 0;
   {
     dim3 g((ctx->max_nsh + 127) / 128, ctx->max_nsh, ctx->nmol);
-    k_blocknorm<<<g, 128, 0, st>>>(xl, ldx, mols, ctx->d_bf.p, ctx->d_sz.p, ctx->d_M.p, ctx->d_flags.p, 1e-12);
+    k_blocknorm<<<g, 128, 0, st>>>(xl, ldx, mols, ctx->d_bf.p, ctx->d_sz.p, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, ctx->d_flags.p, 1e-12);
     CUCHK(cudaGetLastError());
     long long nn = ctx->Mtotal;
     int nb = (int)std::min<long long>((nn + 255) / 256, 1184);
@@ -1915,7 +1924,7 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
   {
     int nthr = 256, wpb = nthr / 32;
     int nb = (ctx->ntask + wpb - 1) / wpb;
-    k_quartets<false><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
+    k_quartets<false><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
                                             ctx->thresh,
                                             cut32, ctx->d_cnt.p, nullptr, nullptr, ctx->d_blkacc.p, 0, 0, 0, 0);
     CUCHK(cudaGetLastError());
@@ -2038,7 +2047,7 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     {
       int nthr = 256, wpb = nthr / 32;
       int nb = (ctx->ntask + wpb - 1) / wpb;
-      k_quartets<true><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
+      k_quartets<true><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
                                              ctx->thresh,
                                              cut32, nullptr, ctx->d_off.p, ctx->d_qlist.p, nullptr, vt0, vt1, obase,
                                              (long long)ctx->d_qlist.n);
