@@ -619,10 +619,27 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
       s_sum[k] = (short)warpmd::hidx(t1 + t2, u1 + u2, v1 + v2);
     }
   }
+  // s_rec[h], h >= 1: the downward recursion R^n_h = P_d R^{n+1}_a + m R^{n+1}_b of Hermite
+  // triple h, packed as a | b << 10 | d << 20 | m << 22 (d = 0, 1, 2 for x, y, z)
+  __shared__ int s_rec[WD::HL];
   for (int k = threadIdx.x; k < WD::HL; k += blockDim.x) {
     int t, u, v;
     warpmd::herm_of(k, t, u, v);
     s_h[k] = t | (u << 4) | (v << 8);
+    int a = 0, b = 0, d = 0, m = 0;
+    if (t > 0) {
+      a = warpmd::hidx(t - 1, u, v);
+      if (t > 1) b = warpmd::hidx(t - 2, u, v), m = t - 1;
+    } else if (u > 0) {
+      d = 1;
+      a = warpmd::hidx(t, u - 1, v);
+      if (u > 1) b = warpmd::hidx(t, u - 2, v), m = u - 1;
+    } else if (v > 0) {
+      d = 2;
+      a = warpmd::hidx(t, u, v - 1);
+      if (v > 1) b = warpmd::hidx(t, u, v - 2), m = v - 1;
+    }
+    s_rec[k] = a | (b << 10) | (d << 20) | (m << 22);
   }
   for (int k = threadIdx.x; k < WD::NCAB; k += blockDim.x) {
     int x0, y0, z0, x1, y1, z1;
@@ -729,18 +746,10 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
             if (h == 0) {
               val = T(fac[n]);
             } else {
-              const int hc = s_h[h];
-              const int t = hc & 15, u = (hc >> 4) & 15, v = hc >> 8;
-              if (t > 0) {
-                val = Xt * prev[warpmd::hidx(t - 1, u, v)];
-                if (t > 1) val += T(t - 1) * prev[warpmd::hidx(t - 2, u, v)];
-              } else if (u > 0) {
-                val = Yt * prev[warpmd::hidx(t, u - 1, v)];
-                if (u > 1) val += T(u - 1) * prev[warpmd::hidx(t, u - 2, v)];
-              } else {
-                val = Zt * prev[warpmd::hidx(t, u, v - 1)];
-                if (v > 1) val += T(v - 1) * prev[warpmd::hidx(t, u, v - 2)];
-              }
+              const int r = s_rec[h];
+              const int dr = (r >> 20) & 3;
+              const T pd = dr == 0 ? Xt : (dr == 1 ? Yt : Zt);
+              val = pd * prev[r & 1023] + T(r >> 22) * prev[(r >> 10) & 1023];
             }
             cur[h] = val;
           }

@@ -56,10 +56,13 @@ struct PairDims {
 template <int LA, int LB, typename T>
 __device__ __forceinline__ void build_E1(T *E, T PA, T PB, T o2p) {
   constexpr int NT = LA + LB + 1;
+#pragma unroll
   for (int k = 0; k < (LA + 1) * (LB + 1) * NT; ++k) E[k] = T(0);
   E[0] = T(1);
   // grow j at i = 0
+#pragma unroll
   for (int j = 1; j <= LB; ++j)
+#pragma unroll
     for (int t = 0; t <= j; ++t) {
       const T *prev = E + (0 * (LB + 1) + (j - 1)) * NT;
       T v = PB * (t <= j - 1 ? prev[t] : T(0));
@@ -67,10 +70,13 @@ __device__ __forceinline__ void build_E1(T *E, T PA, T PB, T o2p) {
       if (t + 1 <= j - 1) v += T(t + 1) * prev[t + 1];
       E[(0 * (LB + 1) + j) * NT + t] = v;
     }
+#pragma unroll
   for (int i = 1; i <= LA; ++i)
+#pragma unroll
     for (int j = 0; j <= LB; ++j) {
       const T *prev = E + ((i - 1) * (LB + 1) + j) * NT;
       const int tm = i - 1 + j;
+#pragma unroll
       for (int t = 0; t <= i + j; ++t) {
         T v = (t <= tm ? PA * prev[t] : T(0));
         if (t > 0 && t - 1 <= tm) v += o2p * prev[t - 1];
