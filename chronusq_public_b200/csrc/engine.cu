@@ -734,7 +734,7 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
         const T Xt = T(X), Yt = T(Y), Zt = T(Z);
         // level L: one entry
         if (lane == 0) cur[0] = T(fac[L]);
-#pragma unroll 1
+#pragma unroll
         for (int n = L - 1; n >= 0; --n) {
           T *t_ = prev;
           prev = cur;
@@ -1421,8 +1421,9 @@ cqg_status cqg_create(cqg_ctx **out, int device) {
     return CQG_ERR_CUDA;
   }
   // Boys table
-  std::vector<double> tab(BOYS_NT * BOYS_NORD);
+  std::vector<double> tab(BOYS_TABLE_SIZE);
   for (int i = 0; i < BOYS_NT; ++i) host_boys_row(BOYS_NORD - 1, (long double)i / 10.0L, &tab[i * BOYS_NORD]);
+  for (int i = 0; i < BOYS_NT; ++i) tab[BOYS_NT * BOYS_NORD + i] = (double)expl(-(long double)i / 10.0L);
   if (ctx->d_boys.reserve(tab.size()) != cudaSuccess ||
       cudaMemcpy(ctx->d_boys.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
     delete ctx;

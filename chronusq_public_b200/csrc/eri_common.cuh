@@ -20,11 +20,27 @@ struct __align__(16) PrimPair {
 //                 F_m = (2T F_{m+1} + e^-T) / (2m+1).
 //  T >= BOYS_TMAX: F_0 = sqrt(pi/T)/2 (erf(sqrt T) = 1 to 2e-17 there), then upward
 //                 recursion F_{m+1} = ((2m+1) F_m - e^-T) / (2T).
-// Table layout: tab[i * BOYS_NORD + n] = F_n(0.1 i), i = 0..BOYS_NT-1.
+// Table layout: tab[i * BOYS_NORD + n] = F_n(0.1 i), i = 0..BOYS_NT-1, followed by
+// tab[BOYS_NT * BOYS_NORD + i] = exp(-0.1 i).
 #define BOYS_TMAX 36.0
 #define BOYS_NT 361
 #define BOYS_NORD 32
 #define BOYS_NTAYLOR 8
+#define BOYS_TABLE_SIZE (BOYS_NT * BOYS_NORD + BOYS_NT)
+
+// e^x for |x| <= 0.05 from its degree-9 Taylor polynomial (remainder < 3e-20 relative).
+__device__ __forceinline__ double exp_small(double x) {
+  double ex = 1.0 / 362880.0;
+  ex = fma(x, ex, 1.0 / 40320.0);
+  ex = fma(x, ex, 1.0 / 5040.0);
+  ex = fma(x, ex, 1.0 / 720.0);
+  ex = fma(x, ex, 1.0 / 120.0);
+  ex = fma(x, ex, 1.0 / 24.0);
+  ex = fma(x, ex, 1.0 / 6.0);
+  ex = fma(x, ex, 0.5);
+  ex = fma(x, ex, 1.0);
+  return fma(x, ex, 1.0);
+}
 
 template <int L>
 __device__ __forceinline__ void boys_eval(double T, const double* __restrict__ tab, double* F) {
@@ -37,7 +53,7 @@ __device__ __forceinline__ void boys_eval(double T, const double* __restrict__ t
     for (int k = BOYS_NTAYLOR; k >= 1; --k) f = __ldg(row + k - 1) + x * f * (1.0 / k);
     F[L] = f;
     if (L > 0) {
-      const double e = exp(-T);
+      const double e = __ldg(tab + BOYS_NT * BOYS_NORD + i) * exp_small(x);
       const double t2 = 2.0 * T;
 #pragma unroll
       for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * (1.0 / (2 * m + 1));
@@ -95,17 +111,7 @@ __device__ __forceinline__ void boys_eval_sm(double T, const double *s, double *
     f = fma(x, f, c01.x);
     F[L] = f;
     if (L > 0) {
-      double ex = 1.0 / 362880.0;
-      ex = fma(x, ex, 1.0 / 40320.0);
-      ex = fma(x, ex, 1.0 / 5040.0);
-      ex = fma(x, ex, 1.0 / 720.0);
-      ex = fma(x, ex, 1.0 / 120.0);
-      ex = fma(x, ex, 1.0 / 24.0);
-      ex = fma(x, ex, 1.0 / 6.0);
-      ex = fma(x, ex, 0.5);
-      ex = fma(x, ex, 1.0);
-      ex = fma(x, ex, 1.0);
-      const double e = c8e.y * ex;
+      const double e = c8e.y * exp_small(x);
       const double t2 = 2.0 * T;
 #pragma unroll
       for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * (1.0 / (2 * m + 1));
