@@ -224,11 +224,16 @@ class BatchSCF:
                     graph = self.B.capture_formPT(P_static, PT_static, warm=False)
                     self.graph_captures = 1
             Pnew = P.clone()
+            active_d = t.as_tensor(active, device=self.dev)
+            conv_d = t.zeros(self.nmol, dtype=t.bool, device=self.dev)
+            for mi in np.nonzero(active)[0]:
+                self.iterations[mi] = it + 1
+            # the group loop only enqueues device work; convergence flags come back once below
             for g in self.groups:
                 gidx = g["idx"]
-                act = t.as_tensor(active[g["members"]], device=self.dev)
-                if not bool(act.any()):
+                if not active[g["members"]].any():
                     continue
+                act = active_d[gidx]
                 Pg = self.gather(P, g)
                 PTg = self.gather(PT, g)
                 E = (Pg * g["H"]).sum((-1, -2)) + 0.25 * (Pg * PTg).sum((-1, -2)) + self.Enuc[gidx]
@@ -256,7 +261,9 @@ class BatchSCF:
                     A[:, :m, m] = -1.0
                     rhs = t.zeros((Bm.shape[0], m + 1), dtype=t.float64, device=self.dev)
                     rhs[:, m] = -1.0
-                    c = t.linalg.solve(A + 1e-14 * t.eye(m + 1, dtype=t.float64, device=self.dev), rhs)[:, :m]
+                    # solve_ex: no host round trip for an error check; a singular system
+                    # gives non-finite c, caught by `ok` below
+                    c = t.linalg.solve_ex(A + 1e-14 * t.eye(m + 1, dtype=t.float64, device=self.dev), rhs)[0][:, :m]
                     ok = t.isfinite(c).all(-1) & (c.abs().amax(-1) < 1e6)
                     Fx = (c[:, :, None, None] * t.stack(g["hist_F"], 1)).sum(1)
                     F = t.where(ok[:, None, None], Fx, F)
@@ -271,16 +278,10 @@ class BatchSCF:
                 Eold[gidx] = t.where(act, E, Eold[gidx])
                 g["damp"] = t.where(dE.abs() < 1e-6, t.zeros_like(damp),
                                     t.where(damp <= 0.0, t.full_like(damp, self.dampParam), damp))
-                conv = (dE.abs() < self.eneTol) & (dP < self.denTol) & act
+                conv_d[gidx] = (dE.abs() < self.eneTol) & (dP < self.denTol) & act
                 Pn = t.where(act[:, None, None], Pn, Pg)
                 self.scatter(Pn, g, Pnew)
-                conv_h = conv.cpu().numpy()
-                act_h = act.cpu().numpy()
-                for k, mi in enumerate(g["members"]):
-                    if act_h[k]:
-                        self.iterations[mi] = it + 1
-                    if conv_h[k]:
-                        active[mi] = False
+            active &= ~conv_d.cpu().numpy()
             P = Pnew
             t.cuda.synchronize(self.dev)
             self.log.append((it, int(active.sum()), time.perf_counter() - t0))
