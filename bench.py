@@ -245,18 +245,22 @@ def scf_compare(mol, bs, thresh, cutoff, sweep=(), autotune=True):
         out["speedup_time_to_1uEh"] = t_plain / t_mixed
     # learned initial density (network trained on this engine's converged cluster densities)
     from chronusq_public_b200.guess_model import PairMLP, default_weights
-    wpath = default_weights(bs.name)
+    wpath, source = default_weights(bs.name), None
+    if wpath is None and default_weights("cc-pvdz"):
+        # no network for this basis: predict in cc-pVDZ and project the density
+        wpath, source = default_weights("cc-pvdz"), "cc-pvdz"
     if wpath:
         net = PairMLP.load(wpath)
         for key, mixed in (("learned_fp64", False), ("mixed_incremental_learned", True)):
             lg = SingleSlater(mol, bs, ints=warm.ints)
-            lg.guess, lg.guess_model = "LEARNED", net
+            lg.guess, lg.guess_model, lg.guess_source_basis = "LEARNED", net, source
             if mixed:
                 lg.precision, lg.fp32_cutoff, lg.incremental = "mixed", cutoff, True
             E = lg.SCF3()
             out[key] = {"energy": E, "abs_dE_vs_fp64": abs(E - E64), "iterations": lg.nSCFIter,
                         "seconds": lg.scf_seconds, "seconds_to_1uEh": lg.time_to(E64, 1e-6),
-                        "guess_used": lg.guess_used, "weights": os.path.basename(wpath)}
+                        "guess_used": lg.guess_used, "weights": os.path.basename(wpath),
+                        "guess_projected_from": source}
         t_learned = out["mixed_incremental_learned"]["seconds_to_1uEh"]
         if t_plain and t_learned:
             out["speedup_time_to_1uEh_mixed_learned"] = t_plain / t_learned

@@ -467,3 +467,27 @@ def predict_densities(model: PairMLP, mols, bss) -> List[np.ndarray]:
 
 def predict_density(model: PairMLP, mol, bs: BasisSet) -> np.ndarray:
     return predict_densities(model, [mol], [bs])[0]
+
+
+def project_density(P_src, bs_src: BasisSet, bs_tgt: BasisSet, device: int = 0):
+    """Carry a density from basis `bs_src` into `bs_tgt` on the same molecule by the
+    overlap projection P_tgt = S_tt^-1 S_ts P_src S_st S_tt^-1 (the density of the
+    projected orbitals; torch tensors on the device).  The overlaps come from the
+    library's one-electron kernel run on the union of the two bases."""
+    import copy
+    import torch
+    from .aointegrals import AOIntegrals
+    u = copy.copy(bs_tgt)
+    u.shells = list(bs_tgt.shells) + list(bs_src.shells)
+    u.map_sh2bf = np.cumsum([0] + [s.size for s in u.shells[:-1]]).astype(np.int64)
+    u.nbasis = bs_tgt.nbasis + bs_src.nbasis
+    u.name = "%s+%s" % (bs_tgt.name, bs_src.name)
+    ints = AOIntegrals(u, device=device, thresholdSchwartz=1e-12)
+    try:
+        S, _, _ = ints.computeAOOneE([], np.zeros((0, 3)), device_out=True)
+    finally:
+        ints.close()
+    nt = bs_tgt.nbasis
+    Ps = torch.as_tensor(P_src, dtype=torch.float64, device=S.device)
+    M = torch.linalg.solve(S[:nt, :nt], S[:nt, nt:])         # S_tt^-1 S_ts
+    return M @ Ps @ M.T

@@ -95,13 +95,15 @@ class SingleSlater:
         self.xHF = -0.5
         self.guess = "SAD"             # "SAD", "CORE" or "LEARNED" (needs guess_model)
         self.guess_model = None
+        self.guess_source_basis = None   # basis the guess network predicts in (None: this one)
         self.guess_used = None
         # mixed precision + incremental (Delta D) Fock build
         self.precision = "fp64"        # "fp64" or "mixed"
         self.fp32_cutoff = 1e-8        # density-weighted Schwarz bound below which a quartet runs in FP32
         self.incremental = False       # build PT_k = PT_{k-1} + G[D_k - D_{k-1}]
         self.nIncFock = 20             # full rebuild period of the incremental build (singleslater.h:468)
-        self.fp64_switch = 1e-5        # DIIS error below which the builds return to full FP64
+        self.fp64_switch = 1e-5        # DIIS error below which the builds return to FP64 (the
+                                       # converged density is then confirmed on a full FP64 build)
         self.n = basis.nbasis
         self.log: List[SCFIteration] = []
         self.fock_builds = 0
@@ -202,9 +204,17 @@ class SingleSlater:
         orthonormal-basis density are occupied, which gives the idempotent density with
         the right electron counts nearest the prediction.  None when the prediction is not
         finite or its Tr(PS) is more than 10 % off the electron count."""
-        from .guess_model import predict_density
+        from .guess_model import predict_density, project_density
         t = self.torch
-        P = t.as_tensor(predict_density(self.guess_model, self.mol, self.basis), dtype=t.float64, device=self.dev)
+        src = self.guess_source_basis
+        if src and src.lower() != self.basis.name.lower():
+            # the network was trained in another basis: predict there, project here
+            bs_src = BasisSet(src, self.mol.atoms, self.mol.coords)
+            P = project_density(predict_density(self.guess_model, self.mol, bs_src), bs_src, self.basis,
+                                self.dev.index)
+        else:
+            P = t.as_tensor(predict_density(self.guess_model, self.mol, self.basis), dtype=t.float64,
+                            device=self.dev)
         ne = float(t.sum(P * self.overlap))
         nel = self.mol.nelectrons
         if not math.isfinite(ne) or abs(ne - nel) > 0.1 * nel:
@@ -262,6 +272,7 @@ class SingleSlater:
         built = None            # (Ps, Pz, PTs, PTz) of the last build, for Delta D
         since_full = 0
         self.phase_switch_iter = None
+        rebuild_pending = False
         self.fp32_quartets = 0
         for it in range(self.maxSCFIter):
             if self.incremental and built is not None and since_full < self.nIncFock:
@@ -290,11 +301,17 @@ class SingleSlater:
             cnorm = max(float(t.linalg.norm(e)) for e in errs)
             fp_converged = cnorm < xsmall
             if mixed_phase and cnorm < self.fp64_switch:
-                # last iterations in FP64, starting from a full rebuild
+                # last iterations in FP64.  Incremental builds continue in FP64 from the
+                # current PT, and the converged density is confirmed on one full FP64 build
+                # (convergence is tested again on it), so the exact rebuild is not paid while
+                # the SCF is still converging.
                 mixed_phase = False
                 self._set_precision(False)
                 self.phase_switch_iter = it
-                built = None
+                if self.incremental:
+                    rebuild_pending = True
+                else:
+                    built = None
             if diis_on:
                 hist_F.append((Fs, Fz))
                 hist_PT.append((PTs, PTz))
@@ -341,6 +358,10 @@ class SingleSlater:
             conv = fp_converged or (abs(dE) < self.eneTol and ps_rms < self.denTol and
                                     (self.isClosedShell or pz_rms < self.denTol))
             Eold = E
+            if conv and rebuild_pending:
+                rebuild_pending = False
+                built = None
+                continue
             if conv:
                 self.converged = True
                 break

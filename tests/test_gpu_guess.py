@@ -142,3 +142,37 @@ def test_trained_guess_needs_fewer_iterations_than_sad():
         b.close()
     assert np.abs(res["sad"][0] - res["learned"][0]).max() < 1e-8
     assert res["learned"][1].mean() < res["sad"][1].mean()
+
+
+WEIGHTS_DZ = os.path.join(os.path.dirname(WEIGHTS), "h2o_cc-pvdz.npz")
+
+
+@pytest.mark.skipif(not os.path.exists(WEIGHTS_DZ), reason="no trained weights committed")
+def test_projected_learned_guess_in_a_larger_basis():
+    """The cc-pVDZ network's density carried into cc-pVTZ by the overlap projection: the
+    projection of a basis onto itself is the identity, and the SCF started from the
+    projected prediction converges to the SAD-started energy within 1e-8 Eh."""
+    import torch
+    from chronusq_public_b200.basis import BasisSet
+    from chronusq_public_b200.guess_model import PairMLP, project_density
+    from chronusq_public_b200.molecule import water_cluster
+    from chronusq_public_b200.scf import SingleSlater
+    mol = water_cluster(2, 21)
+    dz = BasisSet("cc-pvdz", mol.atoms, mol.coords)
+    rng = np.random.default_rng(1)
+    A = rng.normal(size=(dz.nbasis, dz.nbasis))
+    P = A + A.T
+    same = project_density(P, dz, dz)
+    assert torch.abs(same - torch.as_tensor(P, device=same.device)).max().item() < 1e-9
+    tz = BasisSet("cc-pvtz", mol.atoms, mol.coords)
+    net = PairMLP.load(WEIGHTS_DZ)
+    Es = []
+    for g in ("SAD", "LEARNED"):
+        hf = SingleSlater(mol, tz, thresholdSchwartz=1e-12)
+        hf.guess, hf.guess_model, hf.guess_source_basis = g, net, "cc-pvdz"
+        Es.append(hf.SCF3())
+        assert hf.converged
+        if g == "LEARNED":
+            assert hf.guess_used == "LEARNED"
+        hf.close()
+    assert abs(Es[0] - Es[1]) < 1e-8
