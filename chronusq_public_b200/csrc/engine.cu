@@ -1219,14 +1219,16 @@ template <int LA, int LB, int LC, int LD, bool SCHWARZ, typename T>
 static cudaError_t launch_warp(cqg_ctx *ctx, int blk, long long n, long long sbeg, long long send, cudaStream_t st,
                                const DigestGroups &dg, double *Q) {
   if (n == 0) return cudaSuccess;   // n < 0: count unknown on the host (graph mode)
-  static bool attr_set = false;
+  // the attribute belongs to the kernel on each device: set it once per device
+  static bool attr_set[64] = {};
   const size_t per_warp = warp_smem_bytes<LA, LB, LC, LD, T>() / 4;
   const int wpb_max = (int)std::max<size_t>(1, std::min<size_t>(4, (200u * 1024u) / per_warp));
-  if (!attr_set) {
+  const int dev_slot = (ctx->device >= 0 && ctx->device < 64) ? ctx->device : 0;
+  if (!attr_set[dev_slot]) {
     cudaError_t e = cudaFuncSetAttribute(k_eri_jk_warp<LA, LB, LC, LD, SCHWARZ, T>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(per_warp * wpb_max));
     if (e != cudaSuccess) return e;
-    attr_set = true;
+    attr_set[dev_slot] = true;
   }
   int wpb = wpb_max, cta = 16;
   if (!SCHWARZ && ctx->shape_wpb[blk] > 0) wpb = std::min(wpb_max, ctx->shape_wpb[blk]);
