@@ -435,6 +435,10 @@ __device__ __forceinline__ void digest(const double *v, double deg, int a0, int 
         }
       }
     }
+    // Exchange updates go to Gh(c, a), Gh(d, b), Gh(d, a), Gh(c, b): k_finalize adds
+    // (Gh + Gh^T) / 2, so either orientation gives the same result, and with the bra
+    // index (the same across a bra-uniform warp) as the column the lanes' atomics land in
+    // one column of Gh.
     if (dg.sK[g] != 0.0 && valid) {
       double xbd[NB * ND], xac[NA * NC], xbc[NB * NC], xad[NA * ND];
 #pragma unroll
@@ -462,7 +466,7 @@ __device__ __forceinline__ void digest(const double *v, double deg, int a0, int 
           for (int b = 0; b < NB; ++b)
 #pragma unroll
             for (int d = 0; d < ND; ++d) s += xbd[b * ND + d] * v[((a * NB + b) * NC + c) * ND + d];
-          atomicAdd(G + (a0 + a) + (c0 + c) * n, sK * s);
+          atomicAdd(G + (c0 + c) + (a0 + a) * n, sK * s);
         }
 #pragma unroll
       for (int b = 0; b < NB; ++b)
@@ -473,7 +477,7 @@ __device__ __forceinline__ void digest(const double *v, double deg, int a0, int 
           for (int a = 0; a < NA; ++a)
 #pragma unroll
             for (int c = 0; c < NC; ++c) s += xac[a * NC + c] * v[((a * NB + b) * NC + c) * ND + d];
-          atomicAdd(G + (b0 + b) + (d0 + d) * n, sK * s);
+          atomicAdd(G + (d0 + d) + (b0 + b) * n, sK * s);
         }
 #pragma unroll
       for (int a = 0; a < NA; ++a)
@@ -484,7 +488,7 @@ __device__ __forceinline__ void digest(const double *v, double deg, int a0, int 
           for (int b = 0; b < NB; ++b)
 #pragma unroll
             for (int c = 0; c < NC; ++c) s += xbc[b * NC + c] * v[((a * NB + b) * NC + c) * ND + d];
-          atomicAdd(G + (a0 + a) + (d0 + d) * n, sK * s);
+          atomicAdd(G + (d0 + d) + (a0 + a) * n, sK * s);
         }
 #pragma unroll
       for (int b = 0; b < NB; ++b)
@@ -495,7 +499,7 @@ __device__ __forceinline__ void digest(const double *v, double deg, int a0, int 
           for (int a = 0; a < NA; ++a)
 #pragma unroll
             for (int d = 0; d < ND; ++d) s += xad[a * ND + d] * v[((a * NB + b) * NC + c) * ND + d];
-          atomicAdd(G + (b0 + b) + (c0 + c) * n, sK * s);
+          atomicAdd(G + (c0 + c) + (b0 + b) * n, sK * s);
         }
     }
   }
@@ -990,18 +994,20 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
       for (int k = lane; k < NB * NC; k += 32) xbc[k] = __ldg(Xm + (b0 + k / NC) + (c0 + k % NC) * ld);
       for (int k = lane; k < NA * ND; k += 32) xad[k] = __ldg(Xm + (a0 + k / ND) + (d0 + k % ND) * ld);
       __syncwarp();
+      // every update is written with the index that varies fastest across lanes as the
+      // row (k_finalize symmetrises Gh), so a warp's atomics fall on consecutive addresses
       if (dg.sJ[g] != 0.0) {
         for (int k = lane; k < NA * NB; k += 32) {
           const int a = k / NB, b = k % NB;
           double s = 0.0;
           for (int cd = 0; cd < NC * ND; ++cd) s += xdc[cd] * V[k * NC * ND + cd];
-          atomicAdd(G + (a0 + a) + (b0 + b) * n, sJ * s);
+          atomicAdd(G + (b0 + b) + (a0 + a) * n, sJ * s);
         }
         for (int k = lane; k < NC * ND; k += 32) {
           const int c = k / ND, d = k % ND;
           double s = 0.0;
           for (int ab2 = 0; ab2 < NA * NB; ++ab2) s += xba[ab2] * V[ab2 * NC * ND + k];
-          atomicAdd(G + (c0 + c) + (d0 + d) * n, sJ * s);
+          atomicAdd(G + (d0 + d) + (c0 + c) * n, sJ * s);
         }
       }
       if (dg.sK[g] != 0.0) {
@@ -1010,28 +1016,28 @@ __global__ void __launch_bounds__(128) k_eri_jk_warp(const uint2 *__restrict__ q
           double s = 0.0;
           for (int b = 0; b < NB; ++b)
             for (int d = 0; d < ND; ++d) s += xbd[b * ND + d] * V[((a * NB + b) * NC + c) * ND + d];
-          atomicAdd(G + (a0 + a) + (c0 + c) * n, sK * s);
+          atomicAdd(G + (c0 + c) + (a0 + a) * n, sK * s);
         }
         for (int k = lane; k < NB * ND; k += 32) {   // G(b,d) += X(a,c) v
           const int b = k / ND, d = k % ND;
           double s = 0.0;
           for (int a = 0; a < NA; ++a)
             for (int c = 0; c < NC; ++c) s += xac[a * NC + c] * V[((a * NB + b) * NC + c) * ND + d];
-          atomicAdd(G + (b0 + b) + (d0 + d) * n, sK * s);
+          atomicAdd(G + (d0 + d) + (b0 + b) * n, sK * s);
         }
         for (int k = lane; k < NA * ND; k += 32) {   // G(a,d) += X(b,c) v
           const int a = k / ND, d = k % ND;
           double s = 0.0;
           for (int b = 0; b < NB; ++b)
             for (int c = 0; c < NC; ++c) s += xbc[b * NC + c] * V[((a * NB + b) * NC + c) * ND + d];
-          atomicAdd(G + (a0 + a) + (d0 + d) * n, sK * s);
+          atomicAdd(G + (d0 + d) + (a0 + a) * n, sK * s);
         }
         for (int k = lane; k < NB * NC; k += 32) {   // G(b,c) += X(a,d) v
           const int b = k / NC, c = k % NC;
           double s = 0.0;
           for (int a = 0; a < NA; ++a)
             for (int d = 0; d < ND; ++d) s += xad[a * ND + d] * V[((a * NB + b) * NC + c) * ND + d];
-          atomicAdd(G + (b0 + b) + (c0 + c) * n, sK * s);
+          atomicAdd(G + (c0 + c) + (b0 + b) * n, sK * s);
         }
       }
     }
@@ -1062,8 +1068,6 @@ __global__ void k_finalize(const double *__restrict__ Gh0, Mols mols, double *__
   int bx = blockIdx.x * 32, by = blockIdx.y * 32;
   int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
   for (int k = ty; k < 32; k += 8) {
-    int r = bx + tx, c = by + k;   // load Gh(c', r') transposed tile: Gh(by+k, bx+tx)?
-    (void)r; (void)c;
     int rr = by + tx, cc = bx + k;
     tile[k][tx] = (rr < n && cc < n) ? Gh[(size_t)rr + (size_t)cc * n] : 0.0;  // tile[k][tx] = Gh(by+tx, bx+k)
   }
