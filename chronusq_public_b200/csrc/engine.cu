@@ -440,23 +440,25 @@ __device__ __forceinline__ void digest(const double *v, double deg, int a0, int 
     // index (the same across a bra-uniform warp) as the column the lanes' atomics land in
     // one column of Gh.
     if (dg.sK[g] != 0.0 && valid) {
+      // X is symmetric (checked on entry): its exchange blocks are read as X(d, b), X(c, a),
+      // X(c, b), X(d, a), with the bra index (the same across a bra-uniform warp) as the column
       double xbd[NB * ND], xac[NA * NC], xbc[NB * NC], xad[NA * ND];
 #pragma unroll
       for (int b = 0; b < NB; ++b)
 #pragma unroll
-        for (int d = 0; d < ND; ++d) xbd[b * ND + d] = __ldg(X + (b0 + b) + (d0 + d) * ld);
+        for (int d = 0; d < ND; ++d) xbd[b * ND + d] = __ldg(X + (d0 + d) + (b0 + b) * ld);
 #pragma unroll
       for (int a = 0; a < NA; ++a)
 #pragma unroll
-        for (int c = 0; c < NC; ++c) xac[a * NC + c] = __ldg(X + (a0 + a) + (c0 + c) * ld);
+        for (int c = 0; c < NC; ++c) xac[a * NC + c] = __ldg(X + (c0 + c) + (a0 + a) * ld);
 #pragma unroll
       for (int b = 0; b < NB; ++b)
 #pragma unroll
-        for (int c = 0; c < NC; ++c) xbc[b * NC + c] = __ldg(X + (b0 + b) + (c0 + c) * ld);
+        for (int c = 0; c < NC; ++c) xbc[b * NC + c] = __ldg(X + (c0 + c) + (b0 + b) * ld);
 #pragma unroll
       for (int a = 0; a < NA; ++a)
 #pragma unroll
-        for (int d = 0; d < ND; ++d) xad[a * ND + d] = __ldg(X + (a0 + a) + (d0 + d) * ld);
+        for (int d = 0; d < ND; ++d) xad[a * ND + d] = __ldg(X + (d0 + d) + (a0 + a) * ld);
 #pragma unroll
       for (int a = 0; a < NA; ++a)
 #pragma unroll
