@@ -235,7 +235,8 @@ def scf_compare(mol, bs, thresh, cutoff, sweep=(), autotune=True):
         E = mx.SCF3()
         runs["%.0e" % c] = {"energy": E, "abs_dE_vs_fp64": abs(E - E64), "iterations": mx.nSCFIter,
                             "seconds": mx.scf_seconds, "seconds_to_1uEh": mx.time_to(E64, 1e-6),
-                            "fp32_quartets": mx.fp32_quartets, "fp64_switch_iteration": mx.phase_switch_iter}
+                            "fp32_quartets": mx.fp32_quartets, "fp64_switch_iteration": mx.phase_switch_iter,
+                            "mixed_phase_threshold": mx.mixed_threshold}
     out["mixed_incremental"] = runs["%.0e" % cutoff]
     out["mixed_incremental"]["fp32_cutoff"] = cutoff
     if sweep:
@@ -261,6 +262,15 @@ def scf_compare(mol, bs, thresh, cutoff, sweep=(), autotune=True):
                         "seconds": lg.scf_seconds, "seconds_to_1uEh": lg.time_to(E64, 1e-6),
                         "guess_used": lg.guess_used, "weights": os.path.basename(wpath),
                         "guess_projected_from": source}
+        # the same arm with the context's threshold in the mixed phase too: what the relaxed
+        # mixed-phase screening contributes
+        lg = SingleSlater(mol, bs, ints=warm.ints)
+        lg.guess, lg.guess_model, lg.guess_source_basis = "LEARNED", net, source
+        lg.precision, lg.fp32_cutoff, lg.incremental, lg.mixed_threshold = "mixed", cutoff, True, None
+        E = lg.SCF3()
+        out["mixed_incremental_learned_context_threshold"] = {
+            "energy": E, "abs_dE_vs_fp64": abs(E - E64), "iterations": lg.nSCFIter, "seconds": lg.scf_seconds,
+            "seconds_to_1uEh": lg.time_to(E64, 1e-6)}
         t_learned = out["mixed_incremental_learned"]["seconds_to_1uEh"]
         if t_plain and t_learned:
             out["speedup_time_to_1uEh_mixed_learned"] = t_plain / t_learned

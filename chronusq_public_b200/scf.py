@@ -104,6 +104,10 @@ class SingleSlater:
         self.nIncFock = 20             # full rebuild period of the incremental build (singleslater.h:468)
         self.fp64_switch = 1e-5        # DIIS error below which the builds return to FP64 (the
                                        # converged density is then confirmed on a full FP64 build)
+        self.mixed_threshold = 1e-11   # density-weighted Schwarz threshold of the mixed-phase
+                                       # builds (never tighter than the context's; None: the
+                                       # context's threshold throughout)
+        self._base_threshold = None
         self.n = basis.nbasis
         self.log: List[SCFIteration] = []
         self.fock_builds = 0
@@ -121,12 +125,22 @@ class SingleSlater:
         self.Enuc = self.mol.nuclear_repulsion()
 
     # ------------------------------------------------------------------ pieces ---
+    def _mixed_threshold_active(self) -> bool:
+        """True when the mixed phase screens at a looser threshold than the context's."""
+        base = self.ints.thresholdSchwartz if self._base_threshold is None else self._base_threshold
+        return self.mixed_threshold is not None and self.mixed_threshold > base
+
     def _set_precision(self, mixed: bool):
         from .aointegrals import PREC_FP64, PREC_MIXED
+        if self._base_threshold is None:
+            self._base_threshold = self.ints.thresholdSchwartz
         if mixed:
             self.ints.setPrecision(PREC_MIXED, self.fp32_cutoff)
+            if self._mixed_threshold_active():
+                self.ints.thresholdSchwartz = self.mixed_threshold
         else:
             self.ints.setPrecision(PREC_FP64, 0.0)
+            self.ints.thresholdSchwartz = self._base_threshold
 
     def formPT(self, Ps, Pz=None):
         t0 = time.perf_counter()
@@ -273,6 +287,7 @@ class SingleSlater:
         since_full = 0
         self.phase_switch_iter = None
         rebuild_pending = False
+        reset_diis_next = False
         self.fp32_quartets = 0
         for it in range(self.maxSCFIter):
             if self.incremental and built is not None and since_full < self.nIncFock:
@@ -286,6 +301,9 @@ class SingleSlater:
             if mixed_phase:
                 self.fp32_quartets += self.ints.stats()["quartets_fp32"]
             built = (Ps, Pz, PTs, PTz)
+            if reset_diis_next:
+                hist_F, hist_PT, hist_E = [], [], []
+                reset_diis_next = False
             Fs = 2.0 * self.coreH + PTs
             Fz = PTz.clone()
             FOs, FOz = self._ortho(Fs), self._ortho(Fz)
@@ -301,17 +319,23 @@ class SingleSlater:
             cnorm = max(float(t.linalg.norm(e)) for e in errs)
             fp_converged = cnorm < xsmall
             if mixed_phase and cnorm < self.fp64_switch:
-                # last iterations in FP64.  Incremental builds continue in FP64 from the
+                # last iterations in FP64 at the context's threshold.  When the mixed phase
+                # screened at a looser threshold, its PT carries the skipped quartets (about
+                # 1e-7 Eh in the energy at 1e-11): the next build is a full FP64 one and DIIS
+                # restarts from it, so no loose Fock matrix is extrapolated with the exact ones.
+                # Otherwise (FP32 rounding only) incremental builds continue in FP64 from the
                 # current PT, and the converged density is confirmed on one full FP64 build
                 # (convergence is tested again on it), so the exact rebuild is not paid while
                 # the SCF is still converging.
+                loose = self._mixed_threshold_active()
                 mixed_phase = False
                 self._set_precision(False)
                 self.phase_switch_iter = it
-                if self.incremental:
+                if self.incremental and not loose:
                     rebuild_pending = True
                 else:
                     built = None
+                reset_diis_next = loose
             if diis_on:
                 hist_F.append((Fs, Fz))
                 hist_PT.append((PTs, PTz))
@@ -365,6 +389,8 @@ class SingleSlater:
             if conv:
                 self.converged = True
                 break
+        self._set_precision(False)          # the context's own threshold and FP64 again
+        self._base_threshold = None
         self.onePDMScalar, self.onePDMMz = Ps, Pz
         self.totalEnergy = Eold
         self.nSCFIter = len(self.log)

@@ -51,3 +51,32 @@ def test_mixed_incremental_scf_energy_within_1uEh():
     assert abs(E - E64) < 1e-6, (E, E64)
     assert mx.time_to(E64, 1e-6) is not None
     ref.close()
+
+
+def test_mixed_phase_threshold_is_loosened_then_restored():
+    """The mixed phase screens at mixed_threshold (1e-11 here, looser than the context's
+    1e-14); from the FP64 switch on, the builds use the context's threshold again, start
+    from a full rebuild, and the converged energy matches the FP64 one within 1e-8 Eh."""
+    from chronusq_public_b200.scf import SingleSlater
+    mol = water_cluster(3, 2)
+    bs = BasisSet("cc-pvdz", mol.atoms, mol.coords)
+    ref = SingleSlater(mol, bs)
+    E64 = ref.SCF3()
+    seen = []
+    mx = SingleSlater(mol, bs, ints=ref.ints)
+    mx.precision, mx.fp32_cutoff, mx.incremental = "mixed", 1e-8, True
+    assert mx.mixed_threshold == 1e-11
+    E = mx.SCF3(on_iteration=lambda s, rec: seen.append((s.ints.thresholdSchwartz, s.ints.stats()["quartets"])))
+    k = mx.phase_switch_iter
+    assert k is not None and 0 < k < len(seen) - 1
+    assert all(th == 1e-11 for th, _ in seen[:k]) and all(th == 1e-14 for th, _ in seen[k:])
+    assert ref.ints.thresholdSchwartz == 1e-14
+    assert abs(E - E64) < 1e-8, (E, E64)
+    # the switch is decided after iteration k's (mixed) build; iteration k + 1 builds the full
+    # FP64 PT: more quartets than any incremental build before it
+    assert seen[k + 1][1] > max(q for _, q in seen[1:k + 1])
+    # with the context's threshold throughout (mixed_threshold None) the result is the same
+    tight = SingleSlater(mol, bs, ints=ref.ints)
+    tight.precision, tight.fp32_cutoff, tight.incremental, tight.mixed_threshold = "mixed", 1e-8, True, None
+    assert abs(tight.SCF3() - E64) < 1e-8
+    ref.close()
