@@ -214,36 +214,53 @@ def config_of(args, w, bs):
             "launch_shapes": "default" if args.no_autotune else "autotuned in the first warm-up build"}
 
 
-def scf_compare(mol, bs, thresh, cutoff, sweep=(), autotune=True):
-    """Time to converged SCF: plain FP64 GPU build vs mixed precision + incremental build.
-    Times include the SAD guess (atomic SCFs cached beforehand) and every iteration."""
+SCF_ARMS = ("plain", "mixed", "learned", "mixed_learned", "mixed_learned_context")
+
+
+def scf_compare(mol, bs, thresh, cutoff, sweep=(), autotune=True, arms=SCF_ARMS):
+    """Time to converged SCF: plain FP64 GPU build vs mixed precision + incremental build,
+    each with the SAD and the learned guess.  Times include the guess (atomic SCFs cached
+    beforehand) and every iteration.  `arms` picks a subset; without the plain arm, each
+    arm's time to 1 uEh is measured against its own converged energy (the final phase of
+    every arm is FP64 at the context's threshold), and the output says so."""
     from chronusq_public_b200.scf import SingleSlater
     warm = SingleSlater(mol, bs, thresholdSchwartz=thresh)
     Pg, Pzg, _, _ = warm.formGuess()      # atomic SAD densities cached, kernels warm
     if autotune:
         warm.ints.autotune_next()         # launch shapes tuned on one full build, shared by every arm
         warm.formPT(Pg, Pzg)
-    plain = SingleSlater(mol, bs, ints=warm.ints)
-    E64 = plain.SCF3()
-    out = {"plain_fp64": {"energy": E64, "iterations": plain.nSCFIter, "seconds": plain.scf_seconds,
-                          "seconds_to_1uEh": plain.time_to(E64, 1e-6), "fock_builds": plain.fock_builds,
-                          "fock_seconds": plain.fock_seconds}}
-    runs = {}
-    for c in sorted(set([cutoff] + list(sweep))):
-        mx = SingleSlater(mol, bs, ints=warm.ints)
-        mx.precision, mx.fp32_cutoff, mx.incremental = "mixed", c, True
-        E = mx.SCF3()
-        runs["%.0e" % c] = {"energy": E, "abs_dE_vs_fp64": abs(E - E64), "iterations": mx.nSCFIter,
-                            "seconds": mx.scf_seconds, "seconds_to_1uEh": mx.time_to(E64, 1e-6),
-                            "fp32_quartets": mx.fp32_quartets, "fp64_switch_iteration": mx.phase_switch_iter,
-                            "mixed_phase_threshold": mx.mixed_threshold}
-    out["mixed_incremental"] = runs["%.0e" % cutoff]
-    out["mixed_incremental"]["fp32_cutoff"] = cutoff
-    if sweep:
-        out["cutoff_sweep"] = runs
-    t_plain, t_mixed = out["plain_fp64"]["seconds_to_1uEh"], out["mixed_incremental"]["seconds_to_1uEh"]
-    if t_plain and t_mixed:
-        out["speedup_time_to_1uEh"] = t_plain / t_mixed
+    out, E64 = {}, None
+    if "plain" in arms:
+        plain = SingleSlater(mol, bs, ints=warm.ints)
+        E64 = plain.SCF3()
+        out["plain_fp64"] = {"energy": E64, "iterations": plain.nSCFIter, "seconds": plain.scf_seconds,
+                             "seconds_to_1uEh": plain.time_to(E64, 1e-6), "fock_builds": plain.fock_builds,
+                             "fock_seconds": plain.fock_seconds}
+    else:
+        out["reference_energy"] = "each arm's own converged energy (no plain FP64 arm run)"
+
+    def record(hf, E, extra):
+        ref = E if E64 is None else E64
+        r = {"energy": E, "iterations": hf.nSCFIter, "seconds": hf.scf_seconds,
+             "seconds_to_1uEh": hf.time_to(ref, 1e-6)}
+        if E64 is not None:
+            r["abs_dE_vs_fp64"] = abs(E - E64)
+        r.update(extra)
+        return r
+
+    if "mixed" in arms:
+        runs = {}
+        for c in sorted(set([cutoff] + list(sweep))):
+            mx = SingleSlater(mol, bs, ints=warm.ints)
+            mx.precision, mx.fp32_cutoff, mx.incremental = "mixed", c, True
+            E = mx.SCF3()
+            runs["%.0e" % c] = record(mx, E, {"fp32_quartets": mx.fp32_quartets,
+                                              "fp64_switch_iteration": mx.phase_switch_iter,
+                                              "mixed_phase_threshold": mx.mixed_threshold})
+        out["mixed_incremental"] = runs["%.0e" % cutoff]
+        out["mixed_incremental"]["fp32_cutoff"] = cutoff
+        if sweep:
+            out["cutoff_sweep"] = runs
     # learned initial density (network trained on this engine's converged cluster densities)
     from chronusq_public_b200.guess_model import PairMLP, default_weights
     wpath, source = default_weights(bs.name), None
@@ -252,28 +269,27 @@ def scf_compare(mol, bs, thresh, cutoff, sweep=(), autotune=True):
         wpath, source = default_weights("cc-pvdz"), "cc-pvdz"
     if wpath:
         net = PairMLP.load(wpath)
-        for key, mixed in (("learned_fp64", False), ("mixed_incremental_learned", True)):
+        # the last arm keeps the context's threshold in the mixed phase too: what the relaxed
+        # mixed-phase screening contributes
+        for arm, key, mixed, mthr in (("learned", "learned_fp64", False, None),
+                                      ("mixed_learned", "mixed_incremental_learned", True, 1e-11),
+                                      ("mixed_learned_context", "mixed_incremental_learned_context_threshold",
+                                       True, None)):
+            if arm not in arms:
+                continue
             lg = SingleSlater(mol, bs, ints=warm.ints)
             lg.guess, lg.guess_model, lg.guess_source_basis = "LEARNED", net, source
             if mixed:
-                lg.precision, lg.fp32_cutoff, lg.incremental = "mixed", cutoff, True
+                lg.precision, lg.fp32_cutoff, lg.incremental, lg.mixed_threshold = "mixed", cutoff, True, mthr
             E = lg.SCF3()
-            out[key] = {"energy": E, "abs_dE_vs_fp64": abs(E - E64), "iterations": lg.nSCFIter,
-                        "seconds": lg.scf_seconds, "seconds_to_1uEh": lg.time_to(E64, 1e-6),
-                        "guess_used": lg.guess_used, "weights": os.path.basename(wpath),
-                        "guess_projected_from": source}
-        # the same arm with the context's threshold in the mixed phase too: what the relaxed
-        # mixed-phase screening contributes
-        lg = SingleSlater(mol, bs, ints=warm.ints)
-        lg.guess, lg.guess_model, lg.guess_source_basis = "LEARNED", net, source
-        lg.precision, lg.fp32_cutoff, lg.incremental, lg.mixed_threshold = "mixed", cutoff, True, None
-        E = lg.SCF3()
-        out["mixed_incremental_learned_context_threshold"] = {
-            "energy": E, "abs_dE_vs_fp64": abs(E - E64), "iterations": lg.nSCFIter, "seconds": lg.scf_seconds,
-            "seconds_to_1uEh": lg.time_to(E64, 1e-6)}
-        t_learned = out["mixed_incremental_learned"]["seconds_to_1uEh"]
-        if t_plain and t_learned:
-            out["speedup_time_to_1uEh_mixed_learned"] = t_plain / t_learned
+            out[key] = record(lg, E, {"guess_used": lg.guess_used, "weights": os.path.basename(wpath),
+                                      "guess_projected_from": source})
+    t_plain = out.get("plain_fp64", {}).get("seconds_to_1uEh")
+    for key, name in (("mixed_incremental", "speedup_time_to_1uEh"),
+                      ("mixed_incremental_learned", "speedup_time_to_1uEh_mixed_learned")):
+        t = out.get(key, {}).get("seconds_to_1uEh")
+        if t_plain and t:
+            out[name] = t_plain / t
     warm.close()
     return out
 
@@ -294,10 +310,15 @@ def main():
     ap.add_argument("--sweep", action="store_true", help="also sweep the FP32 cutoff 1e-10..1e-6")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes instead of autotuned ones")
+    ap.add_argument("--scf-arms", default=",".join(SCF_ARMS),
+                    help="comma-separated SCF arms to run (%s)" % ", ".join(SCF_ARMS))
     ap.add_argument("--batch", type=int, default=0,
                     help="also run the batched-SCF comparison on this many (H2O)_n, n in 1..24, 6-31G(d)")
     ap.add_argument("--batch-single", type=int, default=64, help="molecules converged one at a time")
     args = ap.parse_args()
+    bad = [a for a in args.scf_arms.split(",") if a not in SCF_ARMS]
+    if bad:
+        ap.error("unknown SCF arm(s): %s" % ", ".join(bad))
     ws, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference(args, ws, rank)
@@ -414,7 +435,7 @@ def main():
         if not args.no_scf:
             line["scf"] = scf_compare(mol, bs, w["thresh"], args.fp32_cutoff,
                                       sweep=(1e-10, 1e-9, 1e-8, 1e-7, 1e-6) if args.sweep else (),
-                                      autotune=not args.no_autotune)
+                                      autotune=not args.no_autotune, arms=args.scf_arms.split(","))
         if args.batch > 0:
             from chronusq_public_b200.workloads import batch_scf_comparison
             line["batch_scf"] = batch_scf_comparison(args.batch, args.batch_single)
