@@ -127,6 +127,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(x: float, pg=None, device="cuda") -> float:
+    """The largest of every rank's `x` (a time: the job ends with its slowest replica);
+    `x` itself on one rank.  `pg` is torch.distributed once initialised, else None."""
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -373,12 +384,8 @@ def main():
         pg.barrier()
     ints.setTiming(False)
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    tot_ms = sum(step_ms)
-    if pg:
-        t = torch.tensor([tot_ms], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        tot_ms = float(t.item())
-    value = ws * sum(quartets) / (tot_ms * 1e-3)
+    tot_ms = max_over_ranks(sum(step_ms), pg)
+    value = ws * sum(quartets) / (tot_ms * 1e-3)      # replicas: every rank builds the same workload
     st_last = ints.stats()
 
     # end to end through the C ABI with pinned host buffers
@@ -395,11 +402,7 @@ def main():
         t1 = time.perf_counter()
         if k >= args.warmup:
             e2e_t.append(t1 - t0)
-    e2e_val = ws * quartets[0] / (sum(e2e_t) / len(e2e_t)) if e2e_t else None
-    if pg and e2e_t:
-        t = torch.tensor([sum(e2e_t)], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_val = ws * quartets[0] * len(e2e_t) / float(t.item())
+    e2e_val = ws * quartets[0] * len(e2e_t) / max_over_ranks(sum(e2e_t), pg) if e2e_t else None
     err = float(np.abs(PTh.numpy() - PT.cpu().numpy()).max()) if e2e_t else None
 
     if rank == 0:
