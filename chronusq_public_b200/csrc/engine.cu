@@ -2211,10 +2211,17 @@ cqg_status cqg_twoe_contract_direct(cqg_ctx *ctx, int nmat, const double *const 
 cqg_status cqg_form_pt(cqg_ctx *ctx, int is_rhf, double xHF, const double *Ps, const double *Pz, double *PTs,
                        double *PTz, int ld, int on_device, void *stream) {
   if (!ctx || !Ps || !PTs || (!is_rhf && (!Pz || !PTz))) return CQG_ERR_BAD_ARG;
-  if (ctx->nshell == 0) return CQG_ERR_STATE;
+  if (ctx->nshell == 0) {
+    ctx->err = "cqg_set_basis has not been called";
+    return CQG_ERR_STATE;
+  }
+  const int n = ctx->nbf;
+  if (ld < n) {   // checked before PT is zeroed: nothing is written on a bad call
+    ctx->err = "leading dimension below the number of basis functions";
+    return CQG_ERR_BAD_ARG;
+  }
   CUCHK(cudaSetDevice(ctx->device));
   cudaStream_t st = (cudaStream_t)stream;
-  const int n = ctx->nbf;
   // PT zeroed first (singleslater_fock.h:47,54)
   if (on_device) {
     CUCHK(cudaMemset2DAsync(PTs, ld * sizeof(double), 0, n * sizeof(double), n, st));

@@ -192,3 +192,19 @@ def test_chunked_quartet_list_matches_single_pass():
     st = ints.stats()
     assert st["chunks"] > 1 and st["quartets"] == n1
     assert np.abs(G2 - G1).max() <= 1e-12
+
+
+def test_form_pt_rejects_short_leading_dimension_before_writing():
+    import ctypes
+    mol = single_water(4)
+    bs = BasisSet("6-31g*", mol.atoms, mol.coords)
+    ints = _aoi()(bs)
+    n = bs.nbasis
+    D = rand_sym(n, 6)
+    PT = np.full((n, n), 7.0, order="F")
+    d = ctypes.c_void_p
+    st = ints._L.cqg_form_pt(ints._ctx, 1, -0.5, d(D.ctypes.data), None, d(PT.ctypes.data), None, n - 1, 0, None)
+    assert st == 1                                   # CQG_ERR_BAD_ARG
+    assert b"leading dimension" in ints._L.cqg_last_error(ints._ctx)
+    assert (PT == 7.0).all()                          # PT not zeroed on the rejected call
+    ints.close()
