@@ -97,6 +97,31 @@ def test_eri_permutational_symmetry():
         assert np.allclose(v, O.eri_quartet(ob, s[2], s[3], s[0], s[1]).transpose(2, 3, 0, 1), atol=1e-13)
 
 
+def test_schwarz_bounds_every_shell_quartet():
+    """Q(a,b) = sqrt(max_ij |(ij|ij)|) over the functions of shell pair (a,b)
+    (builders.cpp:469-517), and the Cauchy-Schwarz inequality |(ab|cd)| <= Q_ab Q_cd that
+    the screen relies on, over every shell quartet of a water molecule."""
+    mol = single_water(3)
+    bs = BasisSet("6-31g*", mol.atoms, mol.coords)
+    ob = O.OracleBasis.from_basis(bs)
+    Q = O.schwarz(ob)
+    eri = O.eri_full(ob)
+    off, sz = ob.offsets, ob.sizes
+    sl = [slice(int(o), int(o + z)) for o, z in zip(off, sz)]
+    assert np.allclose(Q, Q.T, rtol=0, atol=0)
+    for a in range(bs.nshell):
+        for b in range(bs.nshell):
+            blk = eri[sl[a], sl[b], sl[a], sl[b]]
+            diag = np.array([blk[i, j, i, j] for i in range(sz[a]) for j in range(sz[b])])
+            assert abs(Q[a, b] - math.sqrt(np.abs(diag).max())) <= 1e-14 * max(1.0, Q[a, b])
+    for a in range(bs.nshell):
+        for b in range(bs.nshell):
+            for c in range(bs.nshell):
+                m = np.abs(eri[sl[a], sl[b], sl[c], :]).reshape(sz[a] * sz[b] * sz[c], -1)
+                for d in range(bs.nshell):
+                    assert m[:, sl[d]].max() <= Q[a, b] * Q[c, d] * (1 + 1e-12) + 1e-15
+
+
 def test_direct_equals_incore_contraction():
     """newTwoEContractDirect with no screening equals the in-core N^4 contraction
     (contract.h:239-259: COULOMB {i,j,k,l}X{l,k}, EXCHANGE {i,l,k,j}X{l,k}, times 2)."""
