@@ -1,0 +1,112 @@
+"""The C++ change that a ChronusQ maintainer adds (the cpp block of INTEGRATION.md) is
+compiled against stand-ins with the reference's names and signatures, linked to
+libcqgpu.so, and run.  Without a GPU the call reaches cqg_create and reports its failure
+through CErr; with one it completes and gives J of a one-function basis."""
+import os
+import re
+import shutil
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIBDIR = os.path.join(ROOT, "chronusq_public_b200")
+
+# Stand-ins for the reference types the change touches, with the reference's member names:
+# libint2::Shell (alpha, contr[].l/.pure/.coeff, O), BasisSet::nShell() / shells(int)
+# (basisset.h:398, 420), AOIntegrals members nBasis_, thresholdSchwartz_, basisSet_ and the
+# nested ERI_CONTRACTION_TYPE (aointegrals.h:161-173, 468-470), CErr(std::string, ostream&)
+# (cerr.h:30) throwing std::runtime_error as cerr.cpp does.
+PRELUDE = r"""
+#include <array>
+#include <cassert>
+#include <functional>
+#include <iostream>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+namespace libint2 {
+struct Shell {
+  struct Contraction { int l; bool pure; std::vector<double> coeff; };
+  std::vector<double> alpha;
+  std::vector<Contraction> contr;
+  std::array<double, 3> O;
+};
+}
+namespace ChronusQ {
+inline void CErr(std::string m, std::ostream &out = std::cout) { throw std::runtime_error(m); }
+class BasisSet {
+ public:
+  std::vector<libint2::Shell> shells_;
+  inline int nShell() { return this->shells_.size(); }
+  inline libint2::Shell &shells(int i) { return this->shells_[i]; }
+};
+class AOIntegrals {
+ public:
+  int nBasis_ = 0;
+  double thresholdSchwartz_ = 1.0e-14;
+  BasisSet *basisSet_ = nullptr;
+  enum ERI_CONTRACTION_TYPE { COULOMB, EXCHANGE };
+  template <typename Op, typename T>
+  void newTwoEContractDirect(const std::vector<std::reference_wrapper<Op>> &X,
+                             std::vector<std::reference_wrapper<Op>> &AX,
+                             std::vector<ERI_CONTRACTION_TYPE> &contractionList, std::vector<T> &scalingFactors);
+};
+struct RealMatrix {
+  std::vector<double> v;
+  double *data() { return v.data(); }
+};
+}
+"""
+
+MAIN = r"""
+int main() {
+  using namespace ChronusQ;
+  BasisSet bs;
+  // one s function: exponent 1, coefficient of the normalised primitive, at the origin
+  bs.shells_.push_back({{1.0}, {{0, false, {0.7127054703549902}}}, {0.0, 0.0, 0.0}});
+  AOIntegrals ints;
+  ints.basisSet_ = &bs;
+  ints.nBasis_ = 1;
+  RealMatrix X{{1.0}}, AX{{0.0}};
+  std::vector<std::reference_wrapper<RealMatrix>> xs{X}, axs{AX};
+  std::vector<AOIntegrals::ERI_CONTRACTION_TYPE> types{AOIntegrals::COULOMB};
+  std::vector<double> scale{1.0};
+  try {
+    ints.newTwoEContractDirect(xs, axs, types, scale);
+    std::cout.precision(17);
+    std::cout << "ok " << AX.v[0] << "\n";
+  } catch (const std::exception &e) {
+    std::cout << "error: " << e.what() << "\n";
+  }
+  return 0;
+}
+"""
+
+
+def _shim_source():
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    blocks = re.findall(r"```cpp\n(.*?)```", text, re.S)
+    assert len(blocks) == 1
+    return blocks[0]
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="no C++ compiler")
+def test_integration_shim_compiles_links_and_runs(tmp_path):
+    lib = os.path.join(LIBDIR, "libcqgpu.so")
+    if not os.path.exists(lib):
+        pytest.skip("libcqgpu.so not built")
+    src = tmp_path / "shim.cpp"
+    src.write_text(PRELUDE + _shim_source() + MAIN)
+    exe = tmp_path / "shim"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Werror=return-type", str(src), "-o", str(exe),
+                    "-I", os.path.join(ROOT, "include"), "-L", LIBDIR, "-lcqgpu", "-Wl,-rpath," + LIBDIR],
+                   check=True, capture_output=True, text=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True, timeout=120).stdout.strip()
+    if out.startswith("ok"):
+        # (ss|ss) of one normalised s function with exponent 1 is 2 / sqrt(pi); COULOMB gives
+        # AX += 0.5 * scale * 4 J = 2 (ss|ss) X
+        assert abs(float(out.split()[1]) - 2 * 1.1283791670955126) < 1e-12, out
+    else:
+        assert out == "error: cqg_create failed", out
