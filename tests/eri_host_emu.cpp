@@ -1,0 +1,148 @@
+// Test infrastructure: a host (g++) build of the generated per-thread ERI code
+// (csrc/gen_eri.py output, eri_classes.cuh).  The CUDA qualifiers become plain C++ and the
+// few device intrinsics get host definitions, so the same generated arithmetic runs on the
+// CPU and is checked against the oracle without a GPU.  Nothing in the library uses this
+// file; tests/test_eri_host_emu.py compiles it.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+// Compiled with an include directory whose cuda_runtime.h is empty: the definitions the
+// generated code needs from it follow here.
+#define __device__
+#define __host__
+#define __forceinline__ inline
+#define __constant__
+#define __align__(n) alignas(n)
+struct double2 {
+  double x, y;
+};
+struct double3 {
+  double x, y, z;
+};
+struct EmuDim {
+  unsigned x;
+};
+static const EmuDim threadIdx = {0}, blockDim = {1};   // stage_boys fills the whole table
+static inline int __double2int_rn(double x) { return (int)std::nearbyint(x); }   // ties to even
+static inline double rsqrt(double x) { return 1.0 / std::sqrt(x); }
+template <typename T>
+static inline T __ldg(const T *p) {
+  return *p;
+}
+
+#include "eri_classes.cuh"
+
+namespace {
+
+// Boys table in the engine's global layout (cqg_create in csrc/engine.cu):
+// tab[i * BOYS_NORD + n] = F_n(0.1 i), then tab[BOYS_NT * BOYS_NORD + i] = exp(-0.1 i).
+// F_nmax from its series in long double, lower orders by downward recursion.
+std::vector<double> boys_table() {
+  std::vector<double> tab(BOYS_TABLE_SIZE);
+  for (int i = 0; i < BOYS_NT; ++i) {
+    const long double T = (long double)i / 10.0L;
+    const int nmax = BOYS_NORD - 1;
+    long double term = 1.0L / (2 * nmax + 1), sum = term;
+    for (int k = 1; k < 2000; ++k) {
+      term *= 2.0L * T / (2 * nmax + 2 * k + 1);
+      sum += term;
+      if (term < sum * 1e-22L) break;
+    }
+    const long double ex = expl(-T);
+    long double f = ex * sum;
+    tab[i * BOYS_NORD + nmax] = (double)f;
+    for (int m = nmax - 1; m >= 0; --m) {
+      f = (2.0L * T * f + ex) / (2 * m + 1);
+      tab[i * BOYS_NORD + m] = (double)f;
+    }
+    tab[BOYS_NT * BOYS_NORD + i] = (double)ex;
+  }
+  return tab;
+}
+
+// All primitive pairs of two shells (Gaussian product theorem data, PrimPair layout).
+std::vector<PrimPair> prim_pairs(int na, const double *aa, const double *ca, const double *A, int nb,
+                                 const double *ab, const double *cb, const double *B) {
+  const double s2pi52 = std::sqrt(2.0 * std::pow(3.14159265358979323846, 2.5));
+  double AB2 = 0;
+  for (int x = 0; x < 3; ++x) AB2 += (A[x] - B[x]) * (A[x] - B[x]);
+  std::vector<PrimPair> out;
+  for (int i = 0; i < na; ++i)
+    for (int j = 0; j < nb; ++j) {
+      const double al = aa[i], be = ab[j], p = al + be;
+      PrimPair pp;
+      pp.p = p;
+      pp.ip = 1.0 / p;
+      pp.Kp = s2pi52 * ca[i] * cb[j] * std::exp(-al * be / p * AB2) / p;
+      pp.Px = (al * A[0] + be * B[0]) / p;
+      pp.Py = (al * A[1] + be * B[1]) / p;
+      pp.Pz = (al * A[2] + be * B[2]) / p;
+      out.push_back(pp);
+    }
+  return out;
+}
+
+constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+constexpr bool warp_class(int a, int b, int c, int d) {
+  return ncart(a) * ncart(b) * ncart(c) * ncart(d) > 150 || a + b + c + d >= 6;
+}
+
+struct Quartet {
+  const PrimPair *bra, *ket;
+  int nbra, nket;
+  double3 A, B, C, D;
+  double *out;
+};
+
+template <int LA, int LB, int LC, int LD, typename T>
+int call(const Quartet &q) {
+  if constexpr (warp_class(LA, LB, LC, LD)) {
+    return -1;   // evaluated by the warp-cooperative kernel, not by generated code
+  } else {
+    static const std::vector<double> tab = boys_table();
+    alignas(16) static double s[BOYS_NT * BOYS_SROW];
+    stage_boys<LA + LB + LC + LD>(tab.data(), s);
+    constexpr int n = (LA > 1 ? 2 * LA + 1 : ncart(LA)) * (LB > 1 ? 2 * LB + 1 : ncart(LB)) *
+                      (LC > 1 ? 2 * LC + 1 : ncart(LC)) * (LD > 1 ? 2 * LD + 1 : ncart(LD));
+    T v[n];
+    EriClass<LA, LB, LC, LD>::template run<T>(q.bra, q.nbra, q.ket, q.nket, q.A, q.B, q.C, q.D, s, v);
+    for (int k = 0; k < n; ++k) q.out[k] = (double)v[k];
+    return n;
+  }
+}
+
+struct Entry {
+  int la, lb, lc, ld;
+  int (*f64)(const Quartet &);
+  int (*f32)(const Quartet &);
+};
+#define EMU_ENTRY(a, b, c, d, T) Entry{a, b, c, d, &call<a, b, c, d, double>, &call<a, b, c, d, float>}
+const Entry kTable[] = CQG_CLASS_LIST(EMU_ENTRY, double);
+
+}  // namespace
+
+extern "C" {
+
+// One contracted quartet (ab|cd) of class (la lb|lc ld), in the engine's orientation
+// (la >= lb, lc >= ld, bra pair class >= ket pair class).  nprim[4]; alpha/coef: the four
+// shells' exponents and normalised contraction coefficients, concatenated; centers: 4 x 3.
+// out gets the spherical (L > 1) or Cartesian components, row-major [a][b][c][d].
+// fp32 != 0 runs the FP32 instantiation (Boys values FP64, everything after in float).
+// Returns the number of values, or -1 for a class the generated code does not cover.
+int emu_eri(int la, int lb, int lc, int ld, const int *nprim, const double *alpha, const double *coef,
+            const double *centers, int fp32, double *out) {
+  int off[4] = {0, nprim[0], nprim[0] + nprim[1], nprim[0] + nprim[1] + nprim[2]};
+  std::vector<PrimPair> bra = prim_pairs(nprim[0], alpha + off[0], coef + off[0], centers, nprim[1],
+                                         alpha + off[1], coef + off[1], centers + 3);
+  std::vector<PrimPair> ket = prim_pairs(nprim[2], alpha + off[2], coef + off[2], centers + 6, nprim[3],
+                                         alpha + off[3], coef + off[3], centers + 9);
+  Quartet q{bra.data(), ket.data(), (int)bra.size(), (int)ket.size(),
+            {centers[0], centers[1], centers[2]}, {centers[3], centers[4], centers[5]},
+            {centers[6], centers[7], centers[8]}, {centers[9], centers[10], centers[11]}, out};
+  for (const Entry &e : kTable)
+    if (e.la == la && e.lb == lb && e.lc == lc && e.ld == ld) return fp32 ? e.f32(q) : e.f64(q);
+  return -1;
+}
+
+}  // extern "C"

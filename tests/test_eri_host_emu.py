@@ -1,0 +1,121 @@
+"""The generated per-thread ERI code (csrc/gen_eri.py), compiled for the host by g++
+(tests/eri_host_emu.cpp), against the oracle's integrals (oracle/cq_oracle.c) on the CPU.
+
+The GPU parity tests check the same code end to end through the Fock build; this test
+isolates the integral arithmetic of every per-thread class, f shells included, so that a
+change to the generator can be checked without a GPU."""
+import ctypes
+import importlib.util
+import os
+import shutil
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from chronusq_public_b200.basis import BasisSet
+from chronusq_public_b200.molecule import water_cluster
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CSRC = os.path.join(ROOT, "chronusq_public_b200", "csrc")
+
+
+def _gen_module():
+    spec = importlib.util.spec_from_file_location("gen_eri_for_test", os.path.join(CSRC, "gen_eri.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+@pytest.fixture(scope="module")
+def emu(tmp_path_factory):
+    if shutil.which("g++") is None:
+        pytest.skip("no C++ compiler")
+    d = tmp_path_factory.mktemp("eri_emu")
+    (d / "_gen").mkdir()
+    (d / "stub").mkdir()
+    (d / "stub" / "cuda_runtime.h").write_text("// host emulation of the generated code: empty\n")
+    shutil.copy(os.path.join(CSRC, "eri_common.cuh"), d / "eri_common.cuh")
+    subprocess.run([sys.executable, os.path.join(CSRC, "gen_eri.py"), str(d / "_gen" / "eri_classes.cuh"), "3"],
+                   check=True)
+    so = d / "emu.so"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-shared", "-fPIC", "-Wno-unknown-pragmas",
+                    "-I", str(d / "stub"), "-I", str(d / "_gen"), os.path.join(ROOT, "tests", "eri_host_emu.cpp"),
+                    "-o", str(so)], check=True)
+    lib = ctypes.CDLL(str(so))
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int)
+    lib.emu_eri.argtypes = [ctypes.c_int] * 4 + [ip, dp, dp, dp, ctypes.c_int, dp]
+    lib.emu_eri.restype = ctypes.c_int
+    return lib
+
+
+def _run(lib, ob, shells, fp32=False):
+    L = [int(ob.L[s]) for s in shells]
+    off = np.concatenate([[0], np.cumsum(ob.nprim)])
+    nprim = np.array([ob.nprim[s] for s in shells], dtype=np.int32)
+    alpha = np.concatenate([ob.alpha[off[s]:off[s + 1]] for s in shells])
+    coef = np.concatenate([ob.coef[off[s]:off[s + 1]] for s in shells])
+    cen = np.ascontiguousarray(np.concatenate([ob.centers[s] for s in shells]))
+    out = np.zeros(int(np.prod([ob.sizes[s] for s in shells])))
+    dp = ctypes.POINTER(ctypes.c_double)
+    n = lib.emu_eri(*L, nprim.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), alpha.ctypes.data_as(dp),
+                    coef.ctypes.data_as(dp), cen.ctypes.data_as(dp), 1 if fp32 else 0, out.ctypes.data_as(dp))
+    assert n == out.size, (L, n, out.size)
+    return out
+
+
+def _classes():
+    g = _gen_module()
+    return [q for q in g.quartet_classes(3) if q not in g.WARP_CLASSES]
+
+
+def _pick(ob, rng, q):
+    """Random shells of angular momenta q (engine orientation), spread over the atoms."""
+    out = []
+    for l in q:
+        cand = np.flatnonzero(ob.L == l)
+        out.append(int(rng.choice(cand)))
+    return out
+
+
+@pytest.fixture(scope="module")
+def tz():
+    mol = water_cluster(2, 5)
+    return O.OracleBasis.from_basis(BasisSet("cc-pvtz", mol.atoms, mol.coords))
+
+
+@pytest.mark.parametrize("q", _classes(), ids=lambda q: "%d%d%d%d" % q)
+def test_generated_class_matches_oracle(emu, tz, q):
+    rng = np.random.default_rng(sum(10 ** i * l for i, l in enumerate(q)))
+    for _ in range(3):
+        shells = _pick(tz, rng, q)
+        ref = O.eri_quartet(tz, *shells).ravel()
+        got = _run(emu, tz, shells)
+        assert np.abs(got - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max()), (q, shells)
+
+
+@pytest.mark.parametrize("q", [(0, 0, 0, 0), (1, 0, 1, 0), (2, 0, 1, 1), (1, 1, 1, 1)],
+                         ids=lambda q: "%d%d%d%d" % q)
+def test_generated_class_fp32_instantiation(emu, tz, q):
+    rng = np.random.default_rng(7)
+    for _ in range(3):
+        shells = _pick(tz, rng, q)
+        ref = O.eri_quartet(tz, *shells).ravel()
+        got = _run(emu, tz, shells, fp32=True)
+        assert np.abs(got - ref).max() <= 2e-5 * max(1e-3, np.abs(ref).max()), (q, shells)
+
+
+def test_every_per_thread_class_is_covered(emu, tz):
+    """Warp classes are not in the generated code; every other class is."""
+    g = _gen_module()
+    assert len(_classes()) + len(g.WARP_CLASSES) == len(g.quartet_classes(3))
+    for q in g.WARP_CLASSES:
+        dp = ctypes.POINTER(ctypes.c_double)
+        z = np.zeros(1)
+        n = emu.emu_eri(*q, np.array([1, 1, 1, 1], dtype=np.int32).ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                        np.ones(4).ctypes.data_as(dp), np.ones(4).ctypes.data_as(dp),
+                        np.zeros(12).ctypes.data_as(dp), 0, z.ctypes.data_as(dp))
+        assert n == -1, q
