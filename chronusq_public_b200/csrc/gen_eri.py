@@ -176,11 +176,25 @@ def herm_terms(tag, ca, cb):
     return out
 
 
-def _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd):
+def _wname(members, j, m, h, c):
+    return "W%d_%d_%d_%d" % (j, m, h, c) if members else "W%d_%d_%d" % (j, h, c)
+
+
+def _aname(members, mb, mk, i):
+    return "acc%d_%d_%d" % (mb, mk, i) if members else "acc%d" % i
+
+
+def _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members=None):
     """One pass over `nbt` bra primitive pairs starting at bra[ib]: their E coefficients,
     the ket loop (each ket primitive pair loaded and its E coefficients built once for
-    all nbt bra primitives), and the bra transforms into acc."""
+    all nbt bra primitives), and the bra transforms into acc.
+
+    members = (mb, mk) emits the sibling form: the primitive pairs carry unit contraction
+    coefficients, bw[m * nbra + i] / kw[m * nket + i] are member m's coefficient products,
+    and one W per ket member and one acc per (bra member, ket member) are accumulated from
+    the same primitive integrals."""
     L = la + lb + lc + ld
+    mb, mk = members if members else (1, 1)
     needb = {d: set() for d in "xyz"}
     for a in ca:
         for b in cb:
@@ -195,9 +209,10 @@ def _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd):
             g.w("const T %sPA%s = T(pb%d.P%s - A.%s);" % (bt, d, j, d, d))
             g.w("const T %sPB%s = T(pb%d.P%s - B.%s);" % (bt, d, j, d, d))
         emit_E(g, bt, la, lb, needb)
-        for h in range(len(hp)):
-            for c in range(ncd):
-                g.w("T W%d_%d_%d = T(0);" % (j, h, c))
+        for m in range(mk):
+            for h in range(len(hp)):
+                for c in range(ncd):
+                    g.w("T %s = T(0);" % _wname(members, j, m, h, c))
     g.w("PrimPair pk_next;")
     g.w("if (nket > 0) pk_next = ket[0];")
     g.w("for (int ik = 0; ik < nket; ++ik) {")
@@ -206,6 +221,9 @@ def _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd):
     g.w("if (ik + 1 < nket) pk_next = ket[ik + 1];")
     g.w("const double q = pk.p;")
     g.w("const T ko2p = T(0.5 * pk.ip);")
+    if members:
+        for m in range(mk):
+            g.w("const T kw%d = T(kw[%d * nket + ik]);" % (m, m))
     for d in "xyz":
         g.w("const T kPA%s = T(pk.P%s - C.%s);" % (d, d, d))
         g.w("const T kPB%s = T(pk.P%s - D.%s);" % (d, d, d))
@@ -265,15 +283,30 @@ def _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd):
                         expr = "Zpq * %s" % a + ((" + T(%d) * %s" % (v - 1, b)) if b else "")
                     g.w("const T %s%d_%d_%d_%d = %s;" % (r, n, t, u, v, expr))
         # ket transform: W[tuv][cd] += sum_{tau nu phi} (-1)^(..) Ecd * R0_{t+tau,...}
-        for (ci, tnp, cname) in kterms:
-            for hi, (t, u, v) in enumerate(hp):
-                g.w("W%d_%d_%d += %s * %s0_%d_%d_%d;" % (j, hi, ci, cname, r, t + tnp[0], u + tnp[1], v + tnp[2]))
+        if not members:
+            for (ci, tnp, cname) in kterms:
+                for hi, (t, u, v) in enumerate(hp):
+                    g.w("W%d_%d_%d += %s * %s0_%d_%d_%d;" % (j, hi, ci, cname, r, t + tnp[0], u + tnp[1], v + tnp[2]))
+        else:
+            # the ket sum once per (tuv, cd), then one weighted update per ket member
+            for ci in range(ncd):
+                terms = [(tnp, cname) for (cj, tnp, cname) in kterms if cj == ci]
+                for hi, (t, u, v) in enumerate(hp):
+                    expr = " + ".join("%s * %s0_%d_%d_%d" % (cname, r, t + tnp[0], u + tnp[1], v + tnp[2])
+                                      for (tnp, cname) in terms)
+                    g.w("{ const T ks = %s;" % expr)
+                    for m in range(mk):
+                        g.w("  %s += kw%d * ks;" % (_wname(members, j, m, hi, ci), m))
+                    g.w("}")
         g.ind -= 1
         g.w("}")
     g.ind -= 1
     g.w("}")
     # bra transform: acc[ab][cd] += sum_tuv Eab_tuv W[tuv][cd]
     for j in range(nbt):
+        if members:
+            for m in range(mb):
+                g.w("const T bw%d_%d = T(bw[%d * nbra + ib + %d]);" % (j, m, m, j))
         ai = 0
         for a in ca:
             for b in cb:
@@ -281,76 +314,106 @@ def _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd):
                     hi = hidx[tuv]
                     coef = " * ".join(fac) if fac else "T(1)"
                     g.w("{ const T bc = %s;" % coef)
-                    for c in range(ncd):
-                        g.w("  acc%d += bc * W%d_%d_%d;" % (ai * ncd + c, j, hi, c))
+                    if not members:
+                        for c in range(ncd):
+                            g.w("  acc%d += bc * W%d_%d_%d;" % (ai * ncd + c, j, hi, c))
+                    else:
+                        for m1 in range(mb):
+                            g.w("  { const T bcw = bc * bw%d_%d;" % (j, m1))
+                            for m2 in range(mk):
+                                for c in range(ncd):
+                                    g.w("    %s += bcw * %s;" % (_aname(members, m1, m2, ai * ncd + c),
+                                                                _wname(members, j, m2, hi, c)))
+                            g.w("  }")
                     g.w("}")
                 ai += 1
 
 
-def gen_class(la, lb, lc, ld, pa, pb, pc, pd, nbt=1):
+def gen_class(la, lb, lc, ld, pa, pb, pc, pd, nbt=1, members=None):
     """Device function of one class; nbt > 1 walks the bra primitive pairs nbt at a time
     (each ket primitive pair is then read once per nbt bra primitives), with a one-at-a-time
-    loop for the remainder."""
+    loop for the remainder.
+
+    members = (mb, mk) emits eri_gc_<class>_<mb>x<mk> instead: mb bra and mk ket sibling
+    pairs (same centres, angular momenta and exponents, different contraction coefficients)
+    evaluated from one set of primitive integrals.  Its arguments add the coefficient
+    products bw (mb x nbra) and kw (mk x nket) after bra and ket, whose PrimPair Kp carry unit
+    coefficients; out holds mb * mk quartets, member (i, j) at out + (i * mk + j) * n."""
     p_l = la + lb
     ca, cb, cc, cd = cart_list(la), cart_list(lb), cart_list(lc), cart_list(ld)
     nab, ncd = len(ca) * len(cb), len(cc) * len(cd)
     hp = herm_list(p_l)
     hidx = {h: k for k, h in enumerate(hp)}
-    name = "eri_%d%d%d%d" % (la, lb, lc, ld)
+    mb, mk = members if members else (1, 1)
     g = Gen()
     g.lines.append("template <typename T>")
-    g.lines.append("__device__ __forceinline__ void %s(const PrimPair* __restrict__ bra, int nbra,"
-                   " const PrimPair* __restrict__ ket, int nket, double3 A, double3 B, double3 C,"
-                   " double3 D, const double* __restrict__ boys_tab, T* __restrict__ out) {" % name)
-    for i in range(nab * ncd):
-        g.w("T acc%d = T(0);" % i)
+    if not members:
+        name = "eri_%d%d%d%d" % (la, lb, lc, ld)
+        g.lines.append("__device__ __forceinline__ void %s(const PrimPair* __restrict__ bra, int nbra,"
+                       " const PrimPair* __restrict__ ket, int nket, double3 A, double3 B, double3 C,"
+                       " double3 D, const double* __restrict__ boys_tab, T* __restrict__ out) {" % name)
+    else:
+        name = "eri_gc_%d%d%d%d_%dx%d" % (la, lb, lc, ld, mb, mk)
+        g.lines.append("__device__ __forceinline__ void %s(const PrimPair* __restrict__ bra,"
+                       " const double* __restrict__ bw, int nbra, const PrimPair* __restrict__ ket,"
+                       " const double* __restrict__ kw, int nket, double3 A, double3 B, double3 C,"
+                       " double3 D, const double* __restrict__ boys_tab, T* __restrict__ out) {" % name)
+    for m1 in range(mb):
+        for m2 in range(mk):
+            for i in range(nab * ncd):
+                g.w("T %s = T(0);" % _aname(members, m1, m2, i))
     g.w("int ib = 0;")
     if nbt > 1:
         g.w("for (; ib + %d < nbra; ib += %d) {" % (nbt - 1, nbt))
         g.ind += 1
-        _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd)
+        _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members)
         g.ind -= 1
         g.w("}")
     g.w("for (; ib < nbra; ++ib) {")
     g.ind += 1
-    _emit_tile(g, 1, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd)
+    _emit_tile(g, 1, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members)
     g.ind -= 1
     g.w("}")
     # spherical transform, axis by axis: cart arrays named by index tuples
-    dims = [len(ca), len(cb), len(cc), len(cd)]
     pures = [pa, pb, pc, pd]
     ls = [la, lb, lc, ld]
-    cur = {}
-    for idx in itertools.product(*[range(x) for x in dims]):
-        flat = ((idx[0] * dims[1] + idx[1]) * dims[2] + idx[2]) * dims[3] + idx[3]
-        cur[idx] = "acc%d" % flat
-    stage = 0
-    for ax in range(4):
-        if not pures[ax]:
-            continue
-        M = solid_harmonic_matrix(ls[ax])
-        ns = 2 * ls[ax] + 1
-        newdims = list(dims)
-        newdims[ax] = ns
-        new = {}
-        for idx in itertools.product(*[range(x) for x in newdims]):
-            terms = []
-            for k in range(dims[ax]):
-                cval = M[idx[ax], k]
-                if abs(cval) < 1e-15:
+    for m1 in range(mb):
+        for m2 in range(mk):
+            dims = [len(ca), len(cb), len(cc), len(cd)]
+            pre = "m%d_%d_" % (m1, m2) if members else ""
+            cur = {}
+            for idx in itertools.product(*[range(x) for x in dims]):
+                flat = ((idx[0] * dims[1] + idx[1]) * dims[2] + idx[2]) * dims[3] + idx[3]
+                cur[idx] = _aname(members, m1, m2, flat)
+            stage = 0
+            for ax in range(4):
+                if not pures[ax]:
                     continue
-                src = list(idx)
-                src[ax] = k
-                terms.append("%s * %s" % (lit(cval), cur[tuple(src)]))
-            nm = "s%d_%s" % (stage, "_".join(map(str, idx)))
-            g.w("const T %s = %s;" % (nm, " + ".join(terms) if terms else "T(0)"))
-            new[idx] = nm
-        cur = new
-        dims = newdims
-        stage += 1
-    for idx in itertools.product(*[range(x) for x in dims]):
-        flat = ((idx[0] * dims[1] + idx[1]) * dims[2] + idx[2]) * dims[3] + idx[3]
-        g.w("out[%d] = %s;" % (flat, cur[idx]))
+                M = solid_harmonic_matrix(ls[ax])
+                ns = 2 * ls[ax] + 1
+                newdims = list(dims)
+                newdims[ax] = ns
+                new = {}
+                for idx in itertools.product(*[range(x) for x in newdims]):
+                    terms = []
+                    for k in range(dims[ax]):
+                        cval = M[idx[ax], k]
+                        if abs(cval) < 1e-15:
+                            continue
+                        src = list(idx)
+                        src[ax] = k
+                        terms.append("%s * %s" % (lit(cval), cur[tuple(src)]))
+                    nm = "%ss%d_%s" % (pre, stage, "_".join(map(str, idx)))
+                    g.w("const T %s = %s;" % (nm, " + ".join(terms) if terms else "T(0)"))
+                    new[idx] = nm
+                cur = new
+                dims = newdims
+                stage += 1
+            nout = dims[0] * dims[1] * dims[2] * dims[3]
+            base = (m1 * mk + m2) * nout
+            for idx in itertools.product(*[range(x) for x in dims]):
+                flat = ((idx[0] * dims[1] + idx[1]) * dims[2] + idx[2]) * dims[3] + idx[3]
+                g.w("out[%d] = %s;" % (base + flat, cur[idx]))
     g.lines.append("}")
     return name, "\n".join(g.lines)
 
@@ -385,6 +448,30 @@ WARP_CLASSES = {q for q in quartet_classes(3)
 # (ss|ss) 12.3 -> 8.1 ms with 4 at a time; (ps|ss), (ps|ps), (pp|ss), (ds|ss) get 4-15 %
 # slower with 2 (register pressure), so they keep one.
 BRA_TILE = {(0, 0, 0, 0): 4}
+
+
+def members_header(specs):
+    """Header text with the sibling-member variants for `specs` = [(la, lb, lc, ld, mb, mk)],
+    each behind EriClassGC<la, lb, lc, ld, mb, mk>::run, and the list macro CQG_GC_LIST."""
+    parts = ["// GENERATED by gen_eri.py (sibling-member variants) -- do not edit.",
+             "#pragma once",
+             "#include \"../eri_common.cuh\"",
+             "template <int LA, int LB, int LC, int LD, int MB, int MK> struct EriClassGC;",
+             ""]
+    for (la, lb, lc, ld, mb, mk) in specs:
+        name, code = gen_class(la, lb, lc, ld, la > 1, lb > 1, lc > 1, ld > 1,
+                               nbt=BRA_TILE.get((la, lb, lc, ld), 1), members=(mb, mk))
+        parts.append(code)
+        parts.append("template <> struct EriClassGC<%d, %d, %d, %d, %d, %d> {" % (la, lb, lc, ld, mb, mk))
+        parts.append("  template <typename T> static __device__ __forceinline__ void run(const PrimPair* bra,"
+                     " const double* bw, int nbra, const PrimPair* ket, const double* kw, int nket, double3 A,"
+                     " double3 B, double3 C, double3 D, const double* boys_tab, T* out) {")
+        parts.append("    %s<T>(bra, bw, nbra, ket, kw, nket, A, B, C, D, boys_tab, out);" % name)
+        parts.append("  }")
+        parts.append("};")
+        parts.append("")
+    parts.append("#define CQG_GC_LIST(X) {" + ", ".join("X(%d, %d, %d, %d, %d, %d)" % q for q in specs) + "}")
+    return "\n".join(parts) + "\n"
 
 
 def main(path, maxl=2):

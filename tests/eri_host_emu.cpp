@@ -3,6 +3,7 @@
 // few device intrinsics get host definitions, so the same generated arithmetic runs on the
 // CPU and is checked against the oracle without a GPU.  Nothing in the library uses this
 // file; tests/test_eri_host_emu.py compiles it.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -144,5 +145,75 @@ int emu_eri(int la, int lb, int lc, int ld, const int *nprim, const double *alph
     if (e.la == la && e.lb == lb && e.lc == lc && e.ld == ld) return fp32 ? e.f32(q) : e.f64(q);
   return -1;
 }
+
+#ifdef EMU_MEMBERS
+}  // extern "C"
+
+#include "eri_gc_classes.cuh"
+
+namespace {
+
+struct MemberQuartet {
+  const PrimPair *bra, *ket;
+  const double *bw, *kw;
+  int nbra, nket;
+  double3 A, B, C, D;
+  double *out;
+};
+
+template <int LA, int LB, int LC, int LD, int MB, int MK>
+int call_members(const MemberQuartet &q) {
+  static const std::vector<double> tab = boys_table();
+  alignas(16) static double s[BOYS_NT * BOYS_SROW];
+  stage_boys<LA + LB + LC + LD>(tab.data(), s);
+  constexpr int n = (LA > 1 ? 2 * LA + 1 : ncart(LA)) * (LB > 1 ? 2 * LB + 1 : ncart(LB)) *
+                    (LC > 1 ? 2 * LC + 1 : ncart(LC)) * (LD > 1 ? 2 * LD + 1 : ncart(LD));
+  EriClassGC<LA, LB, LC, LD, MB, MK>::template run<double>(q.bra, q.bw, q.nbra, q.ket, q.kw, q.nket, q.A, q.B,
+                                                           q.C, q.D, s, q.out);
+  return n * MB * MK;
+}
+
+struct MemberEntry {
+  int la, lb, lc, ld, mb, mk;
+  int (*f)(const MemberQuartet &);
+};
+#define EMU_MEMBER_ENTRY(a, b, c, d, m, k) MemberEntry{a, b, c, d, m, k, &call_members<a, b, c, d, m, k>}
+const MemberEntry kMemberTable[] = CQG_GC_LIST(EMU_MEMBER_ENTRY);
+
+// Unit-coefficient primitive pairs of two shells, and each member's coefficient products
+// w[m * na * nb + i * nb + j] = ca_m[i] cb_m[j] in the same (i outer, j inner) order.
+std::vector<double> member_weights(int m, int na, const double *ca, int nb, const double *cb) {
+  std::vector<double> w((size_t)m * na * nb);
+  for (int k = 0; k < m; ++k)
+    for (int i = 0; i < na; ++i)
+      for (int j = 0; j < nb; ++j) w[(size_t)k * na * nb + i * nb + j] = ca[k * na + i] * cb[k * nb + j];
+  return w;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Sibling-member quartets: mb bra pairs and mk ket pairs sharing exponents.  alpha holds
+// the four shells' exponents; coef holds, in order, the a coefficients of the mb bra
+// members (mb x na), then b (mb x nb), then c (mk x nc), then d (mk x nd).  out gets the
+// mb * mk quartets, member (i, j) at out + (i * mk + j) * n.
+int emu_eri_members(int la, int lb, int lc, int ld, int mb, int mk, const int *nprim, const double *alpha,
+                    const double *coef, const double *centers, double *out) {
+  const int na = nprim[0], nb = nprim[1], nc = nprim[2], nd = nprim[3];
+  const double *ea = alpha, *eb = ea + na, *ec = eb + nb, *ed = ec + nc;
+  const double *ca = coef, *cb = ca + mb * na, *cc = cb + mb * nb, *cd = cc + mk * nc;
+  std::vector<double> one(std::max(std::max(na, nb), std::max(nc, nd)), 1.0);
+  std::vector<PrimPair> bra = prim_pairs(na, ea, one.data(), centers, nb, eb, one.data(), centers + 3);
+  std::vector<PrimPair> ket = prim_pairs(nc, ec, one.data(), centers + 6, nd, ed, one.data(), centers + 9);
+  std::vector<double> bw = member_weights(mb, na, ca, nb, cb), kw = member_weights(mk, nc, cc, nd, cd);
+  MemberQuartet q{bra.data(), ket.data(), bw.data(), kw.data(), (int)bra.size(), (int)ket.size(),
+                  {centers[0], centers[1], centers[2]}, {centers[3], centers[4], centers[5]},
+                  {centers[6], centers[7], centers[8]}, {centers[9], centers[10], centers[11]}, out};
+  for (const MemberEntry &e : kMemberTable)
+    if (e.la == la && e.lb == lb && e.lc == lc && e.ld == ld && e.mb == mb && e.mk == mk) return e.f(q);
+  return -1;
+}
+#endif
 
 }  // extern "C"

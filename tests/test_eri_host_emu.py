@@ -119,3 +119,74 @@ def test_every_per_thread_class_is_covered(emu, tz):
                         np.ones(4).ctypes.data_as(dp), np.ones(4).ctypes.data_as(dp),
                         np.zeros(12).ctypes.data_as(dp), 0, z.ctypes.data_as(dp))
         assert n == -1, q
+
+
+# sibling-member variants (gen_eri.members_header): one set of primitive integrals serves
+# mb bra and mk ket pairs that share exponents and differ in contraction coefficients
+MEMBER_SPECS = [(0, 0, 0, 0, 3, 3), (0, 0, 0, 0, 2, 4), (1, 0, 0, 0, 2, 3), (1, 0, 1, 0, 2, 2),
+                (1, 1, 0, 0, 3, 1), (2, 0, 0, 0, 1, 2), (2, 0, 1, 1, 2, 2)]
+
+
+@pytest.fixture(scope="module")
+def emu_members(tmp_path_factory):
+    if shutil.which("g++") is None:
+        pytest.skip("no C++ compiler")
+    d = tmp_path_factory.mktemp("eri_emu_members")
+    (d / "_gen").mkdir()
+    (d / "stub").mkdir()
+    (d / "stub" / "cuda_runtime.h").write_text("// host emulation of the generated code: empty\n")
+    shutil.copy(os.path.join(CSRC, "eri_common.cuh"), d / "eri_common.cuh")
+    subprocess.run([sys.executable, os.path.join(CSRC, "gen_eri.py"), str(d / "_gen" / "eri_classes.cuh"), "3"],
+                   check=True)
+    (d / "_gen" / "eri_gc_classes.cuh").write_text(_gen_module().members_header(MEMBER_SPECS))
+    so = d / "emu_members.so"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-shared", "-fPIC", "-Wno-unknown-pragmas", "-DEMU_MEMBERS",
+                    "-I", str(d / "stub"), "-I", str(d / "_gen"), os.path.join(ROOT, "tests", "eri_host_emu.cpp"),
+                    "-o", str(so)], check=True)
+    lib = ctypes.CDLL(str(so))
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.emu_eri_members.argtypes = [ctypes.c_int] * 6 + [ctypes.POINTER(ctypes.c_int), dp, dp, dp, dp]
+    lib.emu_eri_members.restype = ctypes.c_int
+    return lib
+
+
+@pytest.mark.parametrize("spec", MEMBER_SPECS, ids=lambda q: "%d%d%d%d_%dx%d" % q)
+def test_sibling_members_match_separate_quartets(emu_members, tz, spec):
+    """Each member quartet of a sibling evaluation equals the oracle's integral over the
+    contracted functions with that member's coefficients."""
+    la, lb, lc, ld, mb, mk = spec
+    rng = np.random.default_rng(sum(spec))
+    a, b, c, d = _pick(tz, rng, (la, lb, lc, ld))
+    off = np.concatenate([[0], np.cumsum(tz.nprim)])
+    exps = [tz.alpha[off[s]:off[s + 1]] for s in (a, b, c, d)]
+    base = [tz.coef[off[s]:off[s + 1]] for s in (a, b, c, d)]
+    # member 0: the basis' own coefficients; the others: perturbed copies
+    sets = [[base[k] * (1.0 if m == 0 else 1.0 + 0.3 * rng.standard_normal(base[k].size))
+             for m in range(mb if k < 2 else mk)] for k in range(4)]
+    shells_L, shells_n, shells_a, shells_c, shells_R = [], [], [], [], []
+    index = {}
+    for k, s in enumerate((a, b, c, d)):
+        for m, cf in enumerate(sets[k]):
+            index[(k, m)] = len(shells_L)
+            shells_L.append(tz.L[s])
+            shells_n.append(tz.nprim[s])
+            shells_a.append(exps[k])
+            shells_c.append(cf)
+            shells_R.append(tz.centers[s])
+    ob = O.OracleBasis(shells_L, [l > 1 for l in shells_L], shells_n, np.concatenate(shells_a),
+                       np.concatenate(shells_c), np.array(shells_R))
+    nprim = np.array([tz.nprim[s] for s in (a, b, c, d)], dtype=np.int32)
+    coef = np.concatenate([np.concatenate(sets[k]) for k in range(4)])
+    cen = np.ascontiguousarray(np.concatenate([tz.centers[s] for s in (a, b, c, d)]))
+    n = int(np.prod([tz.sizes[s] for s in (a, b, c, d)]))
+    out = np.zeros(n * mb * mk)
+    dp = ctypes.POINTER(ctypes.c_double)
+    got = emu_members.emu_eri_members(la, lb, lc, ld, mb, mk, nprim.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                      np.concatenate(exps).ctypes.data_as(dp), coef.ctypes.data_as(dp),
+                                      cen.ctypes.data_as(dp), out.ctypes.data_as(dp))
+    assert got == out.size
+    for i in range(mb):
+        for j in range(mk):
+            ref = O.eri_quartet(ob, index[(0, i)], index[(1, i)], index[(2, j)], index[(3, j)]).ravel()
+            val = out[(i * mk + j) * n:(i * mk + j + 1) * n]
+            assert np.abs(val - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max()), (spec, i, j)
