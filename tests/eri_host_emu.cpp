@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <utility>
 #include <vector>
 
 // Compiled with an include directory whose cuda_runtime.h is empty: the definitions the
@@ -113,6 +114,29 @@ int call(const Quartet &q) {
   }
 }
 
+template <int L>
+int boys_one(double T, int sm, double *F) {
+  static const std::vector<double> tab = boys_table();
+  alignas(16) static double s[BOYS_NT * BOYS_SROW];
+  static bool staged = false;
+  if (!staged) {
+    stage_boys<L>(tab.data(), s);
+    staged = true;
+  }
+  if (sm)
+    boys_eval_sm<L>(T, s, F);
+  else
+    boys_eval<L>(T, tab.data(), F);
+  return L + 1;
+}
+
+template <int... Ls>
+int boys_dispatch(int L, double T, int sm, double *F, std::integer_sequence<int, Ls...>) {
+  int r = -1;
+  ((L == Ls ? (r = boys_one<Ls>(T, sm, F), 0) : 0), ...);
+  return r;
+}
+
 struct Entry {
   int la, lb, lc, ld;
   int (*f64)(const Quartet &);
@@ -144,6 +168,13 @@ int emu_eri(int la, int lb, int lc, int ld, const int *nprim, const double *alph
   for (const Entry &e : kTable)
     if (e.la == la && e.lb == lb && e.lc == lc && e.ld == ld) return fp32 ? e.f32(q) : e.f64(q);
   return -1;
+}
+
+// The device Boys evaluations for total angular momentum L (0..12): boys_eval_sm on the
+// shared-memory rows of stage_boys<L> (per-thread kernels) when sm != 0, else boys_eval on
+// the global table (warp kernels).  F gets F_0..F_L at T; returns L + 1, or -1.
+int emu_boys(int L, double T, int sm, double *F) {
+  return boys_dispatch(L, T, sm, F, std::make_integer_sequence<int, 13>{});
 }
 
 #ifdef EMU_MEMBERS

@@ -190,3 +190,23 @@ def test_sibling_members_match_separate_quartets(emu_members, tz, spec):
             ref = O.eri_quartet(ob, index[(0, i)], index[(1, i)], index[(2, j)], index[(3, j)]).ravel()
             val = out[(i * mk + j) * n:(i * mk + j + 1) * n]
             assert np.abs(val - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max()), (spec, i, j)
+
+
+@pytest.mark.parametrize("sm", [1, 0], ids=["shared_rows", "global_table"])
+def test_device_boys_against_high_precision(emu, sm):
+    """The device Boys evaluations (Taylor table below T = 36 with e^-T from the degree-9
+    polynomial, asymptotic form and upward recursion above) against the oracle's long-double
+    series, for every total angular momentum to (ff|ff) and T across both branches."""
+    dp = ctypes.POINTER(ctypes.c_double)
+    emu.emu_boys.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, dp]
+    emu.emu_boys.restype = ctypes.c_int
+    Ts = np.concatenate([[0.0, 1e-12, 0.049999, 0.05, 0.05000001, 35.95, 35.999999, 36.0, 36.5, 80.0, 700.0],
+                         np.random.default_rng(3).uniform(0, 40, 300)])
+    worst = 0.0
+    for L in range(13):
+        F = np.zeros(L + 1)
+        for T in Ts:
+            assert emu.emu_boys(L, float(T), sm, F.ctypes.data_as(dp)) == L + 1
+            ref = O.boys(L, float(T))
+            worst = max(worst, float(np.max(np.abs(F - ref) / np.abs(ref))))
+    assert worst < 1e-14, worst        # measured: 2.2e-15
