@@ -102,12 +102,13 @@ class SingleSlater:
         self.fp32_cutoff = 1e-8        # density-weighted Schwarz bound below which a quartet runs in FP32
         self.incremental = False       # build PT_k = PT_{k-1} + G[D_k - D_{k-1}]
         self.nIncFock = 20             # full rebuild period of the incremental build (singleslater.h:468)
-        self.fp64_switch = 1e-5        # DIIS error below which the builds return to FP64 (the
-                                       # converged density is then confirmed on a full FP64 build)
+        self.fp64_switch = 1e-5        # DIIS error below which the builds return to FP64 at the
+                                       # context's threshold (a full FP64 build follows, at the
+                                       # switch or at convergence: see SCF3)
         self.mixed_threshold = 1e-11   # density-weighted Schwarz threshold of the mixed-phase
                                        # builds (never tighter than the context's; None: the
                                        # context's threshold throughout)
-        self._base_threshold = None
+        self._base_threshold = None    # the context's own threshold while an SCF runs
         self.n = basis.nbasis
         self.log: List[SCFIteration] = []
         self.fock_builds = 0
