@@ -698,3 +698,63 @@ void oracle_one_e(int nshell, const int *L, const int *pure, const int *nprim,
     }
   obasis_free(&B);
 }
+
+/* Electric dipole integrals <a| r_k - O_k |b>, k = x, y, z, about origin O, in the
+ * reference basis (each nbf x nbf column-major).  The reference takes them from Libint's
+ * first electric multipole operator (AOIntegrals::elecDipole_, split per component in
+ * AOIntegrals::breakUpMultipole, src/aointegrals/aointegrals_builders.cpp:640-650).  Here:
+ * the 1D Obara-Saika overlap table and x - O_x = (x - B_x) + (B_x - O_x), so the x factor is
+ * S(i, j+1) + (B_x - O_x) S(i, j). */
+void oracle_dipole(int nshell, const int *L, const int *pure, const int *nprim,
+                   const double *alpha, const double *coef, const double *centers,
+                   const double *const *sph, const double *origin, double *Dx, double *Dy, double *Dz) {
+  obasis B; obasis_init(&B, nshell, L, pure, nprim, alpha, coef, centers, sph);
+  size_t nbf = B.nbf;
+  double *outs[3] = {Dx, Dy, Dz};
+#pragma omp parallel for schedule(dynamic)
+  for (int s1 = 0; s1 < nshell; s1++)
+    for (int s2 = 0; s2 < nshell; s2++) {
+      int la = L[s1], lb = L[s2], nca = ncart(la), ncb = ncart(lb);
+      double Mc[3][256];
+      memset(Mc, 0, sizeof(Mc));
+      const double *A = centers + 3 * s1, *Bc = centers + 3 * s2;
+      double AB2 = 0;
+      for (int x = 0; x < 3; x++) AB2 += (A[x] - Bc[x]) * (A[x] - Bc[x]);
+      for (int i = 0; i < nprim[s1]; i++)
+        for (int j = 0; j < nprim[s2]; j++) {
+          double a = alpha[B.poff[s1] + i], b = alpha[B.poff[s2] + j];
+          double ca = coef[B.poff[s1] + i], cb = coef[B.poff[s2] + j];
+          double p = a + b, P[3];
+          for (int x = 0; x < 3; x++) P[x] = (a * A[x] + b * Bc[x]) / p;
+          double pre = exp(-a * b / p * AB2) * ca * cb * pow(PI / p, 1.5);
+          double S1[3][8 * 8];
+          for (int x = 0; x < 3; x++) os_overlap_1d(P[x] - A[x], P[x] - Bc[x], p, la + 1, lb + 2, S1[x], 8);
+          for (int ia = 0; ia < nca; ia++) {
+            int ax[3] = {0, 0, 0};
+            { int c = 0; for (int i1 = 0; i1 <= la; i1++) for (int j1 = 0; j1 <= i1; j1++, c++) if (c == ia) { ax[0] = la - i1; ax[1] = i1 - j1; ax[2] = j1; } }
+            for (int ib = 0; ib < ncb; ib++) {
+              int bx[3] = {0, 0, 0};
+              { int c = 0; for (int i1 = 0; i1 <= lb; i1++) for (int j1 = 0; j1 <= i1; j1++, c++) if (c == ib) { bx[0] = lb - i1; bx[1] = i1 - j1; bx[2] = j1; } }
+              double s[3], d[3];
+              for (int x = 0; x < 3; x++) {
+                s[x] = S1[x][ax[x] * 8 + bx[x]];
+                d[x] = S1[x][ax[x] * 8 + bx[x] + 1] + (Bc[x] - origin[x]) * s[x];
+              }
+              Mc[0][ia * ncb + ib] += pre * d[0] * s[1] * s[2];
+              Mc[1][ia * ncb + ib] += pre * s[0] * d[1] * s[2];
+              Mc[2][ia * ncb + ib] += pre * s[0] * s[1] * d[2];
+            }
+          }
+        }
+      for (int q = 0; q < 3; q++) {
+        double tmp[256], tmp2[256];
+        int d0 = nca, d1 = ncb;
+        memcpy(tmp, Mc[q], sizeof(double) * nca * ncb);
+        if (pure[s1]) { sph_transform_axis(tmp, tmp2, 1, nca, d1, B.sph[la], 2 * la + 1); d0 = 2 * la + 1; memcpy(tmp, tmp2, sizeof(double) * d0 * d1); }
+        if (pure[s2]) { sph_transform_axis(tmp, tmp2, d0, ncb, 1, B.sph[lb], 2 * lb + 1); d1 = 2 * lb + 1; memcpy(tmp, tmp2, sizeof(double) * d0 * d1); }
+        for (int i = 0; i < d0; i++)
+          for (int j = 0; j < d1; j++) outs[q][(B.bfoff[s1] + i) + (size_t)(B.bfoff[s2] + j) * nbf] = tmp[i * d1 + j];
+      }
+    }
+  obasis_free(&B);
+}

@@ -56,6 +56,7 @@ def lib():
             ctypes.c_int, ctypes.c_int]
         _lib.oracle_twoe_contract_direct.restype = ctypes.c_longlong
         _lib.oracle_one_e.argtypes = [ctypes.c_int, i, i, i, d, d, d, pp, ctypes.c_int, d, d, d, d, d]
+        _lib.oracle_dipole.argtypes = [ctypes.c_int, i, i, i, d, d, d, pp, d, d, d, d]
     return _lib
 
 
@@ -223,6 +224,15 @@ def one_e(ob: OracleBasis, charges: Sequence[float], coords: np.ndarray):
     R = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1, 3)
     lib().oracle_one_e(*ob.args(), len(Z), _dp(Z), _dp(R), _dp(S), _dp(T), _dp(V))
     return S, T, V
+
+
+def dipole(ob: OracleBasis, origin=(0.0, 0.0, 0.0)):
+    """Electric dipole integrals <a| r - origin |b> (x, y, z), each nbf x nbf."""
+    n = ob.nbf
+    D = [np.zeros((n, n), order="F") for _ in range(3)]
+    O_ = np.ascontiguousarray(origin, dtype=np.float64)
+    lib().oracle_dipole(*ob.args(), _dp(O_), *[_dp(d) for d in D])
+    return D
 
 
 def form_pt(ob: OracleBasis, Ps: np.ndarray, Pz: np.ndarray = None, xHF: float = -0.5,

@@ -15,6 +15,10 @@ import tarfile
 
 KEEP = ["test0001", "test0002", "test0003", "test0007", "test0008", "test0009",
         "test0010", "test0011", "test0012"]
+# the same molecules in a static electric field (Real RHF 0043-0045 and Real UHF 0049-0054,
+# the field jobs with recorded values): energy and dipole moment (Debye), written to
+# legacy_field_pins.json
+FIELD_KEEP = ["test0043", "test0044", "test0045"] + ["test%04d" % i for i in range(49, 55)]
 
 
 def parse_inp(text):
@@ -43,29 +47,36 @@ def parse_inp(text):
         elif sec == "qm" and "=" in s:
             k, v = [t.strip() for t in s.split("=", 1)]
             out[k.lower()] = v
+        elif sec == "scf" and "=" in s:
+            k, v = [t.strip() for t in s.split("=", 1)]
+            if k.lower() == "field":
+                out["field"] = [float(x) for x in v.split()]
     return out
+
+
+def _pin(tf, rows, t):
+    inp = parse_inp(tf.extractfile("tests/%s_serial_direct.inp" % t).read().decode())
+    basis = {"sto3g.gbs": "sto-3g", "6-31G.gbs": "6-31g", "6-31g.gbs": "6-31g",
+             "cc-pVDZ.gbs": "cc-pvdz", "cc-pvdz.gbs": "cc-pvdz"}.get(inp["basis"], inp["basis"])
+    pin = {"test": t, "energy": float(rows[t][1]), "reference": inp["reference"],
+           "charge": int(inp.get("charge", 0)), "mult": int(inp.get("mult", 1)),
+           "basis": basis, "geom_angstrom": inp["geom"]}
+    if "field" in inp:
+        pin["field"] = inp["field"]
+        pin["dipole_debye"] = [float(x) for x in rows[t][2:5]]
+    return pin
 
 
 def main(tgz):
     tf = tarfile.open(tgz)
     vals = tf.extractfile("tests/chronus-ref.val").read().decode().splitlines()
-    energies = {}
-    for line in vals:
-        f = line.split("/")
-        if f[0] in KEEP:
-            energies[f[0]] = float(f[1])
-    pins = []
-    for t in KEEP:
-        inp = parse_inp(tf.extractfile("tests/%s_serial_direct.inp" % t).read().decode())
-        basis = {"sto3g.gbs": "sto-3g", "6-31G.gbs": "6-31g", "6-31g.gbs": "6-31g",
-                 "cc-pVDZ.gbs": "cc-pvdz", "cc-pvdz.gbs": "cc-pvdz"}.get(inp["basis"], inp["basis"])
-        pins.append({"test": t, "energy": energies[t], "reference": inp["reference"],
-                     "charge": int(inp.get("charge", 0)), "mult": int(inp.get("mult", 1)),
-                     "basis": basis, "geom_angstrom": inp["geom"]})
+    rows = {line.split("/")[0]: line.split("/") for line in vals}
     here = os.path.dirname(os.path.abspath(__file__))
-    with open(os.path.join(here, "legacy_pins.json"), "w") as f:
-        json.dump(pins, f, indent=1)
-    print(json.dumps(pins, indent=1))
+    for name, keep in (("legacy_pins.json", KEEP), ("legacy_field_pins.json", FIELD_KEEP)):
+        pins = [_pin(tf, rows, t) for t in keep]
+        with open(os.path.join(here, name), "w") as f:
+            json.dump(pins, f, indent=1)
+        print(name, len(pins))
 
 
 if __name__ == "__main__":
