@@ -33,7 +33,7 @@ EXPORTED = [
     "cqg_set_basis_batch", "cqg_get_batch_layout", "cqg_twoe_contract_direct_batch", "cqg_one_e_batch",
     "cqg_set_graph_mode", "cqg_graph_status", "cqg_autotune_next", "cqg_get_launch_shapes", "cqg_set_active",
     "cqg_mlp_gemm_bf16", "cqg_mlp_silu_bwd", "cqg_mlp_to_bf16", "cqg_mlp_colsum", "cqg_mlp_mse", "cqg_mlp_adam",
-    "cqg_one_e_noalloc",
+    "cqg_one_e_noalloc", "cqg_dipole",
 ]
 
 
@@ -104,6 +104,7 @@ def load(path: str = LIB_PATH):
     L.cqg_probe_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, d]
     L.cqg_one_e.argtypes = [vp, ctypes.c_int, d, d, vp, vp, vp, ctypes.c_int, ctypes.c_int, vp]
     L.cqg_one_e_noalloc.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_int, vp]
+    L.cqg_dipole.argtypes = [vp, d, vp, ctypes.c_int, ctypes.c_int, vp]
     for name in ["cqg_create", "cqg_destroy", "cqg_set_basis", "cqg_set_threshold", "cqg_set_precision",
                  "cqg_get_schwarz", "cqg_get_sizes", "cqg_twoe_contract_direct", "cqg_form_pt",
                  "cqg_get_stats", "cqg_set_timing", "cqg_probe_fma_peak", "cqg_one_e",
@@ -111,7 +112,7 @@ def load(path: str = LIB_PATH):
                  "cqg_twoe_contract_direct_batch", "cqg_one_e_batch", "cqg_set_graph_mode",
                  "cqg_graph_status", "cqg_autotune_next", "cqg_get_launch_shapes", "cqg_set_active",
                  "cqg_mlp_gemm_bf16", "cqg_mlp_silu_bwd", "cqg_mlp_to_bf16", "cqg_mlp_colsum", "cqg_mlp_mse",
-                 "cqg_mlp_adam", "cqg_one_e_noalloc"]:
+                 "cqg_mlp_adam", "cqg_one_e_noalloc", "cqg_dipole"]:
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

@@ -234,6 +234,26 @@ class AOIntegrals:
         _lib.check(st, self._ctx)
         return S, T, V
 
+    def computeDipole(self, origin=(0.0, 0.0, 0.0), device_out: bool = False):
+        """Electric dipole integrals <mu| r_k - origin_k |nu>, k = x, y, z (the first
+        electric multipoles of AOIntegrals::computeAOOneE, split per component in
+        AOIntegrals::breakUpMultipole, src/aointegrals/aointegrals_builders.cpp:640-650),
+        evaluated on the GPU.  Returns a (3, n, n) CUDA torch tensor when ``device_out``,
+        else a numpy array; each matrix is symmetric."""
+        n = self.nBasis
+        O_ = np.ascontiguousarray(origin, dtype=np.float64)
+        if device_out:
+            import torch
+            D = torch.zeros((3, n, n), dtype=torch.float64, device="cuda:%d" % self.device)
+            ptr, mode = ctypes.c_void_p(D.data_ptr()), 1
+        else:
+            D = np.zeros((3, n, n))
+            ptr, mode = ctypes.c_void_p(D.ctypes.data), 0
+        st = self._L.cqg_dipole(self._ctx, O_.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ptr, n, mode,
+                                self._stream(mode))
+        _lib.check(st, self._ctx)
+        return D
+
     @staticmethod
     def _like(x):
         if _is_torch(x):

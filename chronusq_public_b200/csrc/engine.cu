@@ -2304,6 +2304,51 @@ cqg_status cqg_one_e(cqg_ctx *ctx, int ncharge, const double *Z, const double *R
   return CQG_OK;
 }
 
+cqg_status cqg_dipole(cqg_ctx *ctx, const double *origin, double *D, int ld, int on_device, void *stream) {
+  if (!ctx || !origin || !D) return CQG_ERR_BAD_ARG;
+  if (ctx->nshell == 0) {
+    ctx->err = "cqg_set_basis has not been called";
+    return CQG_ERR_STATE;
+  }
+  if (ctx->nmol != 1) {
+    ctx->err = "cqg_dipole is for single-molecule contexts";
+    return CQG_ERR_STATE;
+  }
+  const int n = ctx->nbf;
+  if (ld < n) {
+    ctx->err = "leading dimension below the number of basis functions";
+    return CQG_ERR_BAD_ARG;
+  }
+  CUCHK(cudaSetDevice(ctx->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  double *dD = D;
+  int ldd = ld;
+  if (!on_device) {
+    if (ctx->d_oe.reserve(3 * (size_t)n * n)) return CQG_ERR_OOM;
+    dD = ctx->d_oe.p;
+    ldd = n;
+  }
+  OneEShells sh;
+  sh.L = ctx->d_shL.p;
+  sh.nprim = ctx->d_shnp.p;
+  sh.poff = ctx->d_shpoff.p;
+  sh.bf = ctx->d_bf.p;
+  sh.alpha = ctx->d_alpha.p;
+  sh.coef = ctx->d_coef.p;
+  sh.center = ctx->d_center.p;
+  const long long np = ctx->nallpairs;
+  k_dipole<<<(unsigned)((np + 63) / 64), 64, 0, st>>>(sh, ctx->d_allpairs.p, np,
+                                                      make_double3(origin[0], origin[1], origin[2]), dD, ldd, n);
+  CUCHK(cudaGetLastError());
+  if (!on_device) {
+    for (int k = 0; k < 3; ++k)
+      CUCHK(cudaMemcpy2DAsync(D + (size_t)k * ld * n, ld * sizeof(double), dD + (size_t)k * n * n,
+                              n * sizeof(double), n * sizeof(double), n, cudaMemcpyDeviceToHost, st));
+    CUCHK(cudaStreamSynchronize(st));
+  }
+  return CQG_OK;
+}
+
 cqg_status cqg_one_e_batch(cqg_ctx *ctx, const int *ncharge_per_mol, const double *Z, const double *R, double *S,
                            double *T, double *V, void *stream) {
   if (!ctx || !ncharge_per_mol || !Z || !R || !S || !T || !V) return CQG_ERR_BAD_ARG;

@@ -209,3 +209,85 @@ __global__ void k_one_e(OneEShells sh, const int2 *__restrict__ pairs, long long
       }
   }
 }
+
+// Electric dipole integrals <a| r_k - O_k |b> (k = x, y, z) of one shell pair, Cartesian
+// blocks Dc[k][ka * ncb + kb].  McMurchie-Davidson first moment (Helgaker, Jorgensen & Olsen
+// eq. 9.5.43): the x factor is sqrt(pi/p) (E^{ij}_1 + (P_x - O_x) E^{ij}_0), the y and z
+// factors are overlaps.  The reference takes these from Libint's first electric multipole
+// operator about the origin (AOIntegrals::elecDipoleSep_, aointegrals_builders.cpp:640-650).
+__device__ __forceinline__ void oe_dipole_pair(const OneEShells &sh, int a, int b, double3 O, double Dc[3][100]) {
+  const int la = sh.L[a], lb = sh.L[b];
+  const int nca = (la + 1) * (la + 2) / 2, ncb = (lb + 1) * (lb + 2) / 2;
+  const double3 A = sh.center[a], B = sh.center[b];
+  const double ABx = A.x - B.x, ABy = A.y - B.y, ABz = A.z - B.z;
+  const double AB2 = ABx * ABx + ABy * ABy + ABz * ABz;
+  for (int k = 0; k < 3; ++k)
+    for (int i = 0; i < nca * ncb; ++i) Dc[k][i] = 0.0;
+  double Ex[OE_MAXL + 1][OE_MAXL + 3][OE_NT], Ey[OE_MAXL + 1][OE_MAXL + 3][OE_NT], Ez[OE_MAXL + 1][OE_MAXL + 3][OE_NT];
+  const double pi = 3.141592653589793;
+  for (int i = 0; i < sh.nprim[a]; ++i)
+    for (int j = 0; j < sh.nprim[b]; ++j) {
+      const double al = sh.alpha[sh.poff[a] + i], be = sh.alpha[sh.poff[b] + j];
+      const double p = al + be, o2p = 0.5 / p;
+      const double K = sh.coef[sh.poff[a] + i] * sh.coef[sh.poff[b] + j] * exp(-al * be / p * AB2);
+      const double Px = (al * A.x + be * B.x) / p, Py = (al * A.y + be * B.y) / p, Pz = (al * A.z + be * B.z) / p;
+      oe_build_E(Ex, la, lb, Px - A.x, Px - B.x, o2p);
+      oe_build_E(Ey, la, lb, Py - A.y, Py - B.y, o2p);
+      oe_build_E(Ez, la, lb, Pz - A.z, Pz - B.z, o2p);
+      const double s1 = sqrt(pi / p);
+      const double pre = K * s1 * s1 * s1;
+      for (int ka = 0; ka < nca; ++ka) {
+        int ax, ay, az;
+        oe_cart(la, ka, ax, ay, az);
+        for (int kb = 0; kb < ncb; ++kb) {
+          int bx, by, bz;
+          oe_cart(lb, kb, bx, by, bz);
+          const double sx = Ex[ax][bx][0], sy = Ey[ay][by][0], sz = Ez[az][bz][0];
+          const double mx = Ex[ax][bx][1] + (Px - O.x) * sx;
+          const double my = Ey[ay][by][1] + (Py - O.y) * sy;
+          const double mz = Ez[az][bz][1] + (Pz - O.z) * sz;
+          Dc[0][ka * ncb + kb] += pre * mx * sy * sz;
+          Dc[1][ka * ncb + kb] += pre * sx * my * sz;
+          Dc[2][ka * ncb + kb] += pre * sx * sy * mz;
+        }
+      }
+    }
+}
+
+// Cartesian block M[ka * ncb + kb] of shell pair (a, b) to real solid harmonics for pure
+// (L > 1) shells, stored at rows a0.., columns b0.. of out and, transposed, at rows b0..,
+// columns a0.. (column-major, leading dimension ld).
+__device__ __forceinline__ void oe_store_pair(const double *M, int la, int lb, int a0, int b0, double *out, int ld) {
+  const int nca = (la + 1) * (la + 2) / 2, ncb = (lb + 1) * (lb + 2) / 2;
+  const int pa = la > 1, pb = lb > 1;
+  const int na = pa ? 2 * la + 1 : nca, nb = pb ? 2 * lb + 1 : ncb;
+  const double *Ca = la == 2 ? kSph2 : kSph3, *Cb = lb == 2 ? kSph2 : kSph3;
+  for (int i = 0; i < na; ++i)
+    for (int j = 0; j < nb; ++j) {
+      double s = 0.0;
+      for (int ka = 0; ka < nca; ++ka) {
+        const double ca = pa ? Ca[i * nca + ka] : (ka == i ? 1.0 : 0.0);
+        if (ca == 0.0) continue;
+        for (int kb = 0; kb < ncb; ++kb) {
+          const double cb = pb ? Cb[j * ncb + kb] : (kb == j ? 1.0 : 0.0);
+          if (cb == 0.0) continue;
+          s += ca * cb * M[ka * ncb + kb];
+        }
+      }
+      out[(size_t)(a0 + i) + (size_t)(b0 + j) * ld] = s;
+      out[(size_t)(b0 + j) + (size_t)(a0 + i) * ld] = s;
+    }
+}
+
+// Dipole integrals of one molecule, one thread per shell pair (a >= b); D0 holds the x, y
+// and z matrices at D0, D0 + ld * nbf and D0 + 2 * ld * nbf.
+__global__ void k_dipole(OneEShells sh, const int2 *__restrict__ pairs, long long npairs, double3 O, double *D0,
+                         int ld, int nbf) {
+  const long long ip = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (ip >= npairs) return;
+  const int a = pairs[ip].x, b = pairs[ip].y;
+  double Dc[3][100];
+  oe_dipole_pair(sh, a, b, O, Dc);
+  for (int k = 0; k < 3; ++k)
+    oe_store_pair(Dc[k], sh.L[a], sh.L[b], sh.bf[a], sh.bf[b], D0 + (size_t)k * ld * nbf, ld);
+}

@@ -12,8 +12,8 @@ keyword tables in src/python/src/parse/meta/knownKeywords.py) with the standard
 * ``[BASIS]``     BASIS (a .gbs name such as STO-3G, 6-31G*, cc-pVDZ), FORCECART (only
   false is handled: the engine evaluates pure shells for l > 1).
 * ``[SCF]``       DENTOL, ENETOL, MAXITER, GUESS (SAD, CORE, LEARNED), DIIS (parseQM.py
-  parseSCF); FIELD, ITP and DT are rejected.  A one-atom molecule uses the CORE guess,
-  as parseSCF does.
+  parseSCF), FIELD (a static field, a.u.: SingleSlater.setField); ITP and DT are
+  rejected.  A one-atom molecule uses the CORE guess, as parseSCF does.
 * ``[MISC]``, ``[INTS]``  accepted and ignored (thread counts and the integral algorithm
   have no meaning here).
 
@@ -138,7 +138,9 @@ def parse_job(text: str) -> Job:
     if bas.get("FORCECART", False):
         raise InputError("Basis.forceCart = true is not handled (pure shells for l > 1 only)")
     scf = sec.get("SCF", {})
-    for k in ("FIELD", "ITP", "DT"):
+    if "FIELD" in scf and len(scf["FIELD"]) != 3:
+        raise InputError("SCF.Field needs three components, got %d" % len(scf["FIELD"]))
+    for k in ("ITP", "DT"):
         if k in scf and (k != "ITP" or scf[k]):
             raise InputError("SCF.%s is not handled by this engine" % k)
     symbols, coords = _geometry(str(mol_s["GEOM"]))
@@ -172,6 +174,8 @@ def run_job(job: Job, device: int = 0, thresholdSchwartz: float = 1e-14, guess_m
         hf.guess = g
     if job.molecule.natoms == 1:
         hf.guess = "CORE"
+    if "FIELD" in s:
+        hf.setField(s["FIELD"])
     if hf.guess == "LEARNED":
         from .guess_model import PairMLP, default_weights
         if guess_model is None:

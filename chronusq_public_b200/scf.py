@@ -65,7 +65,7 @@ class SingleSlater:
     """RHF / UHF SCF on one GPU (reference names kept where they exist)."""
 
     def __init__(self, mol: Molecule, basis: BasisSet, ref: str = "RHF", device: int = 0,
-                 thresholdSchwartz: float = 1e-14, ints: Optional[AOIntegrals] = None):
+                 thresholdSchwartz: float = 1e-14, ints: Optional[AOIntegrals] = None, field=None):
         import torch
         self.torch = torch
         self.mol = mol
@@ -113,17 +113,54 @@ class SingleSlater:
         self.log: List[SCFIteration] = []
         self.fock_builds = 0
         self.fock_seconds = 0.0
+        self.elecField = None          # static electric field (a.u.), None: no field
         self._one_e()
+        if field is not None:
+            self.setField(field)
 
     # ------------------------------------------------------------------ setup ---
     def _one_e(self):
         t = self.torch
         S, T, V = self.ints.computeAOOneE(self.mol.atoms, self.mol.coords, device_out=True)
         self.overlap = S
-        self.coreH = T + V
+        self._H0 = T + V
+        self.coreH = self._H0
         w, U = t.linalg.eigh(S)
         self.X = (U * w.rsqrt()) @ U.T          # Loewdin S^-1/2 (symmetric)
         self.Enuc = self.mol.nuclear_repulsion()
+
+    def setField(self, field):
+        """Static electric field F (a.u., origin 0) for the SCF (SingleSlater::setField,
+        singleslater.h:633-637).  The one-electron Hamiltonian becomes h + F.<r> and the
+        energy gains -F.mu_nuc: the reference subtracts F times its dipole integrals, which
+        carry the electron's charge, from the Fock matrix (AOIntegrals::subElecDipole,
+        aointegrals.h:505-510) and adds F.mu to the energy (singleslater_properties.h:95-101).
+        A zero field is no field, as in the reference.  The SAD atoms see no field (the
+        reference's setField call for them is commented out, singleslater_guess.h:185)."""
+        F = None if field is None else [float(x) for x in field]
+        if F is not None and len(F) != 3:
+            raise ValueError("the field has three components")
+        if F is not None and not any(F):
+            F = None
+        self.elecField = F
+        self.coreH = self._H0
+        self.Enuc = self.mol.nuclear_repulsion()
+        if F is not None:
+            D = self.ints.computeDipole(device_out=True)
+            self.coreH = self._H0 + F[0] * D[0] + F[1] * D[1] + F[2] * D[2]
+            self.Enuc -= float(np.dot(F, self._nuclear_dipole()))
+
+    def _nuclear_dipole(self) -> np.ndarray:
+        Z = np.asarray(self.mol.atoms, dtype=np.float64)
+        return Z @ np.asarray(self.mol.coords, dtype=np.float64).reshape(-1, 3)
+
+    def dipoleMoment(self) -> np.ndarray:
+        """Dipole moment (a.u., origin 0) of the current density: sum_A Z_A R_A - Tr(Ps <r>)
+        (SingleSlater::computeMultipole, singleslater_properties.h:115-130)."""
+        D = self.ints.computeDipole(device_out=True)
+        Ps = self.onePDMScalar
+        el = [float(self.torch.sum(Ps * D[k])) for k in range(3)]
+        return self._nuclear_dipole() - np.asarray(el)
 
     # ------------------------------------------------------------------ pieces ---
     def _mixed_threshold_active(self) -> bool:

@@ -122,6 +122,15 @@ cqg_status cqg_form_pt(cqg_ctx *ctx, int is_rhf, double xHF, const double *Ps,
 cqg_status cqg_one_e(cqg_ctx *ctx, int ncharge, const double *Z, const double *R, double *S,
                      double *T, double *V, int ld, int on_device, void *stream);
 
+/* Electric dipole integrals <mu| r_k - origin_k |nu>, k = x, y, z, of a single-molecule
+ * context: D holds the three nbf x nbf matrices (column-major, leading dimension ld) at D,
+ * D + ld * nbf and D + 2 * ld * nbf, host or device memory as `on_device` says.  Replaces
+ * the first electric multipole integrals of AOIntegrals::computeAOOneE
+ * (AOIntegrals::elecDipole_, split per component in AOIntegrals::breakUpMultipole,
+ * src/aointegrals/aointegrals_builders.cpp:640-650), which SingleSlater adds to the Fock
+ * matrix in a static field (AOIntegrals::subElecDipole, include/aointegrals.h:505-510). */
+cqg_status cqg_dipole(cqg_ctx *ctx, const double *origin, double *D, int ld, int on_device, void *stream);
+
 /* cqg_one_e without any allocation: the same integrals and kernel as cqg_one_e with device
  * S, T, V (leading dimension ld), but the point-charge table is held in a fixed
  * module-scope device array of CQG_ONE_E_NOALLOC_MAX_CHARGES entries (4 doubles each,

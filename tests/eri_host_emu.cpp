@@ -13,6 +13,7 @@
 // generated code needs from it follow here.
 #define __device__
 #define __host__
+#define __global__ static inline   // the kernels compile but are not called here
 #define __forceinline__ inline
 #define __constant__
 #define __align__(n) alignas(n)
@@ -22,10 +23,13 @@ struct double2 {
 struct double3 {
   double x, y, z;
 };
+struct int2 {
+  int x, y;
+};
 struct EmuDim {
   unsigned x;
 };
-static const EmuDim threadIdx = {0}, blockDim = {1};   // stage_boys fills the whole table
+static const EmuDim threadIdx = {0}, blockDim = {1}, blockIdx = {0};   // stage_boys fills the whole table
 static inline int __double2int_rn(double x) { return (int)std::nearbyint(x); }   // ties to even
 static inline double rsqrt(double x) { return 1.0 / std::sqrt(x); }
 template <typename T>
@@ -34,6 +38,7 @@ static inline T __ldg(const T *p) {
 }
 
 #include "eri_classes.cuh"
+#include "one_e.cuh"
 
 namespace {
 
@@ -175,6 +180,30 @@ int emu_eri(int la, int lb, int lc, int ld, const int *nprim, const double *alph
 // the global table (warp kernels).  F gets F_0..F_L at T; returns L + 1, or -1.
 int emu_boys(int L, double T, int sm, double *F) {
   return boys_dispatch(L, T, sm, F, std::make_integer_sequence<int, 13>{});
+}
+
+// The one-electron dipole device code (oe_dipole_pair + oe_store_pair of one_e.cuh) over
+// every shell pair a >= b of a basis: D gets the x, y, z matrices (nbf x nbf each,
+// column-major, consecutive).  bf[s] is shell s's first basis function.
+void emu_dipole(int nshell, const int *L, const int *nprim, const int *poff, const int *bf, const double *alpha,
+                const double *coef, const double *centers, const double *origin, int nbf, double *D) {
+  std::vector<double3> cen(nshell);
+  for (int s = 0; s < nshell; ++s) cen[s] = {centers[3 * s], centers[3 * s + 1], centers[3 * s + 2]};
+  OneEShells sh;
+  sh.L = L;
+  sh.nprim = nprim;
+  sh.poff = poff;
+  sh.bf = bf;
+  sh.alpha = alpha;
+  sh.coef = coef;
+  sh.center = cen.data();
+  const double3 O = {origin[0], origin[1], origin[2]};
+  for (int a = 0; a < nshell; ++a)
+    for (int b = 0; b <= a; ++b) {
+      double Dc[3][100];
+      oe_dipole_pair(sh, a, b, O, Dc);
+      for (int k = 0; k < 3; ++k) oe_store_pair(Dc[k], L[a], L[b], bf[a], bf[b], D + (size_t)k * nbf * nbf, nbf);
+    }
 }
 
 #ifdef EMU_MEMBERS

@@ -38,11 +38,13 @@ def emu(tmp_path_factory):
     (d / "stub").mkdir()
     (d / "stub" / "cuda_runtime.h").write_text("// host emulation of the generated code: empty\n")
     shutil.copy(os.path.join(CSRC, "eri_common.cuh"), d / "eri_common.cuh")
+    shutil.copy(os.path.join(CSRC, "one_e.cuh"), d / "one_e.cuh")
     subprocess.run([sys.executable, os.path.join(CSRC, "gen_eri.py"), str(d / "_gen" / "eri_classes.cuh"), "3"],
                    check=True)
     so = d / "emu.so"
     subprocess.run(["g++", "-std=c++17", "-O1", "-shared", "-fPIC", "-Wno-unknown-pragmas",
-                    "-I", str(d / "stub"), "-I", str(d / "_gen"), os.path.join(ROOT, "tests", "eri_host_emu.cpp"),
+                    "-I", str(d / "stub"), "-I", str(d / "_gen"), "-I", str(d),
+                    os.path.join(ROOT, "tests", "eri_host_emu.cpp"),
                     "-o", str(so)], check=True)
     lib = ctypes.CDLL(str(so))
     dp = ctypes.POINTER(ctypes.c_double)
@@ -136,12 +138,14 @@ def emu_members(tmp_path_factory):
     (d / "stub").mkdir()
     (d / "stub" / "cuda_runtime.h").write_text("// host emulation of the generated code: empty\n")
     shutil.copy(os.path.join(CSRC, "eri_common.cuh"), d / "eri_common.cuh")
+    shutil.copy(os.path.join(CSRC, "one_e.cuh"), d / "one_e.cuh")
     subprocess.run([sys.executable, os.path.join(CSRC, "gen_eri.py"), str(d / "_gen" / "eri_classes.cuh"), "3"],
                    check=True)
     (d / "_gen" / "eri_gc_classes.cuh").write_text(_gen_module().members_header(MEMBER_SPECS))
     so = d / "emu_members.so"
     subprocess.run(["g++", "-std=c++17", "-O1", "-shared", "-fPIC", "-Wno-unknown-pragmas", "-DEMU_MEMBERS",
-                    "-I", str(d / "stub"), "-I", str(d / "_gen"), os.path.join(ROOT, "tests", "eri_host_emu.cpp"),
+                    "-I", str(d / "stub"), "-I", str(d / "_gen"), "-I", str(d),
+                    os.path.join(ROOT, "tests", "eri_host_emu.cpp"),
                     "-o", str(so)], check=True)
     lib = ctypes.CDLL(str(so))
     dp = ctypes.POINTER(ctypes.c_double)
@@ -210,3 +214,29 @@ def test_device_boys_against_high_precision(emu, sm):
             ref = O.boys(L, float(T))
             worst = max(worst, float(np.max(np.abs(F - ref) / np.abs(ref))))
     assert worst < 1e-14, worst        # measured: 2.2e-15
+
+
+@pytest.mark.parametrize("basis", ["6-31g*", "cc-pvtz"])
+def test_device_dipole_integrals_match_oracle(emu, basis):
+    """The dipole device code of one_e.cuh (k_dipole's per-pair work) against the oracle's
+    dipole integrals, about the origin and about a shifted origin."""
+    mol = water_cluster(2, 5)
+    ob = O.OracleBasis.from_basis(BasisSet(basis, mol.atoms, mol.coords))
+    n = ob.nbf
+    poff = np.concatenate([[0], np.cumsum(ob.nprim)[:-1]]).astype(np.int32)
+    bf = np.asarray(ob.offsets, dtype=np.int32)
+    ip = ctypes.POINTER(ctypes.c_int)
+    dp = ctypes.POINTER(ctypes.c_double)
+    emu.emu_dipole.argtypes = [ctypes.c_int, ip, ip, ip, ip, dp, dp, dp, dp, ctypes.c_int, dp]
+    emu.emu_dipole.restype = None
+    for origin in ((0.0, 0.0, 0.0), (0.4, -1.1, 2.3)):
+        o = np.asarray(origin)
+        D = np.zeros(3 * n * n)
+        emu.emu_dipole(ob.nshell, ob.L.ctypes.data_as(ip), ob.nprim.ctypes.data_as(ip), poff.ctypes.data_as(ip),
+                       bf.ctypes.data_as(ip), ob.alpha.ctypes.data_as(dp), ob.coef.ctypes.data_as(dp),
+                       np.ascontiguousarray(ob.centers).ctypes.data_as(dp), o.ctypes.data_as(dp), n,
+                       D.ctypes.data_as(dp))
+        ref = O.dipole(ob, origin)
+        for k in range(3):
+            got = D[k * n * n:(k + 1) * n * n].reshape(n, n, order="F")
+            assert np.abs(got - ref[k]).max() < 1e-12, (basis, origin, k)

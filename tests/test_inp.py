@@ -29,6 +29,11 @@ def test_parse_water_job():
     assert job.scf == {"ENETOL": 1e-9, "DENTOL": 1e-7, "MAXITER": 64, "DIIS": True}
 
 
+def test_field_is_read():
+    job = inp.parse_job(make_input(PINS[0], "field = 0.01 0.0 -0.002\n"))
+    assert job.scf["FIELD"] == [0.01, 0.0, -0.002]
+
+
 def test_isotope_column_and_case_insensitive_keys():
     text = make_input(PINS[0]).replace(" O  ", " O 16").replace("charge", "CHARGE")
     job = inp.parse_job(text)
@@ -39,7 +44,7 @@ def test_isotope_column_and_case_insensitive_keys():
     (("job = SCF", "job = RT"), "SCF only"),
     (("reference = Real RHF", "reference = Real B3LYP"), "Hartree-Fock"),
     (("reference = Real RHF", "reference = Complex RHF"), "complex"),
-    (("[SCF]\n", "[SCF]\nfield = 0 0 0.01\n"), "FIELD"),
+    (("[SCF]\n", "[SCF]\nfield = 0 0.01\n"), "three components"),
     (("[SCF]\n", "[SCF]\nbogus = 1\n"), "not recognized"),
     (("basis = STO-3G", "basis = STO-3G\nforceCart = true"), "forceCart"),
     (("mult = 1\n", ""), "MULT"),
@@ -58,4 +63,23 @@ def test_input_jobs_reproduce_recorded_energies(pin):
     hf = inp.run_job(job)
     assert hf.converged
     assert abs(hf.totalEnergy - pin["energy"]) < 1e-8, (hf.totalEnergy, pin["energy"])
+    hf.close()
+
+
+FIELD_PINS = json.load(open(os.path.join(HERE, "golden", "legacy_field_pins.json")))
+DEBYE = 0.393430307      # e bohr per Debye (the reference's phys.debye)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pin", FIELD_PINS, ids=lambda p: p["test"])
+def test_field_jobs_reproduce_recorded_energies_and_dipoles(pin):
+    """Field jobs (SCF.FIELD) through the input runner: the reference's recorded energies
+    within 1e-8 Eh and dipole moments within 5e-5 relative (Debye)."""
+    job = inp.parse_job(make_input(pin, "field = %r %r %r\n" % tuple(pin["field"])))
+    hf = inp.run_job(job)
+    assert hf.converged
+    assert abs(hf.totalEnergy - pin["energy"]) < 1e-8, (hf.totalEnergy, pin["energy"])
+    mu = hf.dipoleMoment() / DEBYE
+    ref = np.asarray(pin["dipole_debye"])
+    assert np.abs(mu - ref).max() < 5e-5 * max(1.0, np.abs(ref).max()), (mu, ref)
     hf.close()
