@@ -31,6 +31,13 @@ Fock builds through :class:`~chronusq_public_b200.aointegrals.AOIntegrals`:
   projected on its natural orbitals, falling back to SAD when the prediction is
   unphysical; the converged energy does not depend on the guess.
 
+* Static electric field (setField; singleslater_fock.h:215, aointegrals.h:505-510,
+  singleslater_properties.h:95-101): h + F.<r> and E_nuc - F.mu_nuc, origin 0.
+* Mixed precision (no reference counterpart): FP32 quartets below ``fp32_cutoff``,
+  incremental Delta-D builds and a looser screen (``mixed_threshold``) until the DIIS
+  error falls below ``fp64_switch``; then FP64 at the context's threshold, from a full
+  rebuild, so the converged energy is the FP64 one.
+
 The per-iteration HDF5 traffic of the reference (writeSCFFiles, scfutils.h:1114-1188) has
 no counterpart: all state stays in device memory.
 """
