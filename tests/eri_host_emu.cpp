@@ -128,8 +128,10 @@ int boys_one(double T, int sm, double *F) {
     stage_boys<L>(tab.data(), s);
     staged = true;
   }
-  if (sm)
+  if (sm == 1)
     boys_eval_sm<L>(T, s, F);
+  else if (sm == 2)
+    boys_eval_rt(L, T, tab.data(), F);
   else
     boys_eval<L>(T, tab.data(), F);
   return L + 1;
@@ -176,8 +178,9 @@ int emu_eri(int la, int lb, int lc, int ld, const int *nprim, const double *alph
 }
 
 // The device Boys evaluations for total angular momentum L (0..12): boys_eval_sm on the
-// shared-memory rows of stage_boys<L> (per-thread kernels) when sm != 0, else boys_eval on
-// the global table (warp kernels).  F gets F_0..F_L at T; returns L + 1, or -1.
+// shared-memory rows of stage_boys<L> (per-thread kernels) when sm == 1, boys_eval_rt
+// (runtime L, one-electron kernel) when sm == 2, else boys_eval on the global table (warp
+// kernels).  F gets F_0..F_L at T; returns L + 1, or -1.
 int emu_boys(int L, double T, int sm, double *F) {
   return boys_dispatch(L, T, sm, F, std::make_integer_sequence<int, 13>{});
 }

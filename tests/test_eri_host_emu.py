@@ -196,7 +196,7 @@ def test_sibling_members_match_separate_quartets(emu_members, tz, spec):
             assert np.abs(val - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max()), (spec, i, j)
 
 
-@pytest.mark.parametrize("sm", [1, 0], ids=["shared_rows", "global_table"])
+@pytest.mark.parametrize("sm", [1, 0, 2], ids=["shared_rows", "global_table", "runtime_L"])
 def test_device_boys_against_high_precision(emu, sm):
     """The device Boys evaluations (Taylor table below T = 36 with e^-T from the degree-9
     polynomial, asymptotic form and upward recursion above) against the oracle's long-double
