@@ -29,7 +29,9 @@ struct int2 {
 struct EmuDim {
   unsigned x;
 };
-static const EmuDim threadIdx = {0}, blockDim = {1}, blockIdx = {0};   // stage_boys fills the whole table
+// one thread per block: stage_boys fills the whole table, and a kernel body is run for
+// thread index ip by setting blockIdx.x = ip
+static EmuDim threadIdx = {0}, blockDim = {1}, blockIdx = {0};
 static inline int __double2int_rn(double x) { return (int)std::nearbyint(x); }   // ties to even
 static inline double rsqrt(double x) { return 1.0 / std::sqrt(x); }
 template <typename T>
@@ -207,6 +209,35 @@ void emu_dipole(int nshell, const int *L, const int *nprim, const int *poff, con
       oe_dipole_pair(sh, a, b, O, Dc);
       for (int k = 0; k < 3; ++k) oe_store_pair(Dc[k], L[a], L[b], bf[a], bf[b], D + (size_t)k * nbf * nbf, nbf);
     }
+}
+
+// The one-electron kernel body (k_one_e) run for every shell pair a >= b of one molecule:
+// S, T, V (nbf x nbf each, column-major) for point charges Zc at Rc (ncharge x 3).
+void emu_one_e(int nshell, const int *L, const int *nprim, const int *poff, const int *bf, const double *alpha,
+               const double *coef, const double *centers, int ncharge, const double *Zc, const double *Rc, int nbf,
+               double *S, double *T, double *V) {
+  static const std::vector<double> tab = boys_table();
+  std::vector<double3> cen(nshell), rc(ncharge);
+  for (int s = 0; s < nshell; ++s) cen[s] = {centers[3 * s], centers[3 * s + 1], centers[3 * s + 2]};
+  for (int c = 0; c < ncharge; ++c) rc[c] = {Rc[3 * c], Rc[3 * c + 1], Rc[3 * c + 2]};
+  std::vector<int2> pairs;
+  for (int a = 0; a < nshell; ++a)
+    for (int b = 0; b <= a; ++b) pairs.push_back({a, b});
+  OneEShells sh;
+  sh.L = L;
+  sh.nprim = nprim;
+  sh.poff = poff;
+  sh.bf = bf;
+  sh.alpha = alpha;
+  sh.coef = coef;
+  sh.center = cen.data();
+  OneEMols om;
+  std::memset(&om, 0, sizeof(om));
+  for (size_t ip = 0; ip < pairs.size(); ++ip) {
+    blockIdx.x = (unsigned)ip;
+    k_one_e(sh, pairs.data(), (long long)pairs.size(), ncharge, Zc, rc.data(), tab.data(), S, T, V, nbf, om);
+  }
+  blockIdx.x = 0;
 }
 
 #ifdef EMU_MEMBERS

@@ -240,3 +240,30 @@ def test_device_dipole_integrals_match_oracle(emu, basis):
         for k in range(3):
             got = D[k * n * n:(k + 1) * n * n].reshape(n, n, order="F")
             assert np.abs(got - ref[k]).max() < 1e-12, (basis, origin, k)
+
+
+@pytest.mark.parametrize("basis", ["6-31g*", "cc-pvtz"])
+def test_one_electron_kernel_body_matches_oracle(emu, basis):
+    """k_one_e's per-pair work (S, T, V by McMurchie-Davidson) against the oracle's
+    Obara-Saika one-electron integrals, with the nuclei and extra point charges."""
+    mol = water_cluster(2, 5)
+    ob = O.OracleBasis.from_basis(BasisSet(basis, mol.atoms, mol.coords))
+    n = ob.nbf
+    rng = np.random.default_rng(4)
+    R = np.asarray(mol.coords, dtype=np.float64).reshape(-1, 3)
+    Z = np.concatenate([np.asarray(mol.atoms, dtype=np.float64), rng.uniform(-1, 1, 5)])
+    R = np.ascontiguousarray(np.concatenate([R, rng.uniform(-3, 3, (5, 3))]))
+    poff = np.concatenate([[0], np.cumsum(ob.nprim)[:-1]]).astype(np.int32)
+    bf = np.asarray(ob.offsets, dtype=np.int32)
+    ip = ctypes.POINTER(ctypes.c_int)
+    dp = ctypes.POINTER(ctypes.c_double)
+    emu.emu_one_e.argtypes = [ctypes.c_int, ip, ip, ip, ip, dp, dp, dp, ctypes.c_int, dp, dp, ctypes.c_int, dp, dp, dp]
+    emu.emu_one_e.restype = None
+    out = [np.zeros((n, n), order="F") for _ in range(3)]
+    emu.emu_one_e(ob.nshell, ob.L.ctypes.data_as(ip), ob.nprim.ctypes.data_as(ip), poff.ctypes.data_as(ip),
+                  bf.ctypes.data_as(ip), ob.alpha.ctypes.data_as(dp), ob.coef.ctypes.data_as(dp),
+                  np.ascontiguousarray(ob.centers).ctypes.data_as(dp), len(Z), Z.ctypes.data_as(dp),
+                  R.ctypes.data_as(dp), n, *[x.ctypes.data_as(dp) for x in out])
+    ref = O.one_e(ob, Z, R)
+    for name, got, want in zip("STV", out, ref):
+        assert np.abs(got - want).max() < 1e-11 * max(1.0, np.abs(want).max()), (basis, name)
