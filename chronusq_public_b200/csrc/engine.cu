@@ -1194,6 +1194,7 @@ struct cqg_ctx {
   cudaEvent_t ev[4 + 2 * 55];
   bool events = false;
   cqg_stats stats;
+  double *oe_table = nullptr;   // device address of the fixed charge table (cqg_one_e_noalloc)
 };
 
 static double host_boys_row(int nmax, long double T, double *F) {
@@ -2548,29 +2549,22 @@ cqg_status cqg_probe_fma_peak(int device, int fp64, double ms_target, double *tf
 
 // ---- One-electron integrals that allocate nothing ---------------------------------------
 // The point-charge table lives in a fixed module-scope device array instead of the
-// context's growable buffer; its device address is resolved once per device.
-#include <mutex>
-
+// context's growable buffer.  Its device address is resolved on the first such call of a
+// context, with the context's device current, and kept in the context: a context never
+// outlives its device's CUDA context (a cudaDeviceReset frees every buffer a context holds,
+// so it is destroyed and created again), which keeps the address from going stale.
 namespace {
-constexpr int kNoAllocMaxDevices = 64;
 // Z[0..n) followed by R[n..4n) (x, y, z per charge), as k_one_e reads it
 __device__ __align__(256) double g_oe_charge_table[4 * CQG_ONE_E_NOALLOC_MAX_CHARGES];
-std::mutex g_oe_table_mutex;
-double *g_oe_table_addr[kNoAllocMaxDevices] = {};
 
 // With ctx->device current: the device address of g_oe_charge_table on that device.
 cqg_status oe_charge_table(cqg_ctx *ctx, double **out) {
-  if (ctx->device < 0 || ctx->device >= kNoAllocMaxDevices) {
-    ctx->err = "cqg_one_e_noalloc: device ordinal out of range";
-    return CQG_ERR_BAD_ARG;
-  }
-  std::lock_guard<std::mutex> lock(g_oe_table_mutex);
-  if (!g_oe_table_addr[ctx->device]) {
+  if (!ctx->oe_table) {
     void *p = nullptr;
     CUCHK(cudaGetSymbolAddress(&p, g_oe_charge_table));
-    g_oe_table_addr[ctx->device] = (double *)p;
+    ctx->oe_table = (double *)p;
   }
-  *out = g_oe_table_addr[ctx->device];
+  *out = ctx->oe_table;
   return CQG_OK;
 }
 }  // namespace
@@ -2592,7 +2586,10 @@ cqg_status cqg_one_e_noalloc(cqg_ctx *ctx, int ncharge, const double *Z, const d
     ctx->err = "cqg_one_e_noalloc is for single-molecule contexts";
     return CQG_ERR_STATE;
   }
-  if (ld < ctx->nbf) return CQG_ERR_BAD_ARG;
+  if (ld < ctx->nbf) {
+    ctx->err = "leading dimension below the number of basis functions";
+    return CQG_ERR_BAD_ARG;
+  }
   CUCHK(cudaSetDevice(ctx->device));
   double *tab = nullptr;
   const cqg_status s = oe_charge_table(ctx, &tab);

@@ -136,13 +136,17 @@ cqg_status cqg_dipole(cqg_ctx *ctx, const double *origin, double *D, int ld, int
  * module-scope device array of CQG_ONE_E_NOALLOC_MAX_CHARGES entries (4 doubles each,
  * 128 KiB) instead of context scratch, so the call makes no cudaMalloc/cudaFree and calls
  * no allocating library.  Z and R may be host or device pointers; work is enqueued on
- * `stream`, nothing is synchronised.  ncharge > CQG_ONE_E_NOALLOC_MAX_CHARGES returns
- * CQG_ERR_BAD_ARG (cqg_last_error says why).  Nothing has to start at zero: the table is
- * written in full for the entries read and every element of S, T, V is written.
- * The first call on a device resolves the array's device address (cudaGetSymbolAddress,
- * with that device current); make that first call before any stream capture.  The array is
- * shared by every context on a device: calls that overlap (other streams, threads or
- * contexts on the same device) race on it and must be serialised by the caller.
+ * `stream`, nothing is synchronised: pinned or device Z/R are read when the stream reaches
+ * the copy, so keep them alive until then; under stream capture pass device or pinned Z/R
+ * (a pageable host copy cannot be captured).  ncharge > CQG_ONE_E_NOALLOC_MAX_CHARGES and
+ * ld < nbf return CQG_ERR_BAD_ARG (cqg_last_error says why) before anything is written.
+ * Nothing has to start at zero: the table is written in full for the entries read and
+ * every element of the nbf x nbf blocks of S, T, V is written (rows nbf..ld-1 are not).
+ * The first call on a context resolves the array's device address (cudaGetSymbolAddress,
+ * with the context's device current) and keeps it in the context; make that first call
+ * before any stream capture.  The array is shared by every context on a device: calls that
+ * overlap (other streams, threads or contexts on the same device) race on it and must be
+ * serialised by the caller.
  * This entry point has no counterpart in the reference. */
 #define CQG_ONE_E_NOALLOC_MAX_CHARGES 4096
 cqg_status cqg_one_e_noalloc(cqg_ctx *ctx, int ncharge, const double *Z, const double *R,

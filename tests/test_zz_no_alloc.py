@@ -1,6 +1,10 @@
 """cqg_one_e_noalloc (one-electron integrals with a fixed module-scope charge table, no
 allocation) against the allocating entry point cqg_one_e, both called through the C-ABI.
 
+The entry point serves callers that cannot allocate device memory once they run: a host
+program whose own memory pool already holds the GPU, or a loop that must not take the
+device-wide synchronisation a cudaMalloc/cudaFree brings.
+
 Named to be collected last, so it runs both after every other test and alone."""
 import ctypes
 
@@ -36,48 +40,62 @@ def _allocating(ai, Z, R, out, stream):
     _lib.check(st, ai._ctx)
 
 
-def _no_alloc(ai, nq, zp, rp, out, stream):
+def _no_alloc(ai, nq, zp, rp, out, stream, ld=None):
     return ai._L.cqg_one_e_noalloc(ai._ctx, nq, ctypes.c_void_p(zp), ctypes.c_void_p(rp),
-                                   *[ctypes.c_void_p(x.data_ptr()) for x in out], ai.nBasis, stream)
+                                   *[ctypes.c_void_p(x.data_ptr()) for x in out],
+                                   ai.nBasis if ld is None else ld, stream)
 
 
 @pytest.mark.parametrize("basis", ["6-31g*", "cc-pvdz"])
 def test_no_alloc_matches_allocating_entry_point(basis):
+    """Two calls in a row on a fresh context (host charges, then device charges with a
+    padded leading dimension) match cqg_one_e, and neither call changes the device's free
+    memory: the first call, which resolves the table's address, included."""
     import torch
     from chronusq_public_b200.aointegrals import AOIntegrals
     mol = water_cluster(2, 9)
     bs = BasisSet(basis, mol.atoms, mol.coords)
     ai = AOIntegrals(bs)
     n = ai.nBasis
+    ldp = n + 3
     dev = torch.device("cuda", 0)
     stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
     cases = [_charges(mol, 0, 1), _charges(mol, 300, 2)]
-    # every buffer both calls need, allocated before the calls
+    # every buffer both calls need, allocated before the calls; the second call writes into
+    # column-major n x n blocks of ldp x n arrays (stored as n rows of ldp in torch)
     ref = [[torch.zeros((n, n), dtype=torch.float64, device=dev) for _ in range(3)] for _ in cases]
-    got = [[torch.full((n, n), float("nan"), dtype=torch.float64, device=dev) for _ in range(3)] for _ in cases]
+    got0 = [torch.full((n, n), float("nan"), dtype=torch.float64, device=dev) for _ in range(3)]
+    got1 = [torch.full((n, ldp), float("nan"), dtype=torch.float64, device=dev) for _ in range(3)]
     Zd = torch.tensor(cases[1][0], device=dev)
     Rd = torch.tensor(cases[1][1], device=dev)
     for (Z, R), out in zip(cases, ref):
         _allocating(ai, Z, R, out, stream)
     torch.cuda.synchronize(dev)
 
-    # two calls in a row: host charges first, device charges second
     Z0, R0 = cases[0]
-    assert _no_alloc(ai, len(Z0), Z0.ctypes.data, R0.ctypes.data, got[0], stream) == 0, ai._L.cqg_last_error(ai._ctx)
-    torch.cuda.synchronize(dev)
     free0 = torch.cuda.mem_get_info(dev)[0]
-    assert _no_alloc(ai, len(cases[1][0]), Zd.data_ptr(), Rd.data_ptr(), got[1], stream) == 0
+    assert _no_alloc(ai, len(Z0), Z0.ctypes.data, R0.ctypes.data, got0, stream) == 0, ai._L.cqg_last_error(ai._ctx)
+    torch.cuda.synchronize(dev)
+    assert torch.cuda.mem_get_info(dev)[0] == free0
+    assert _no_alloc(ai, len(cases[1][0]), Zd.data_ptr(), Rd.data_ptr(), got1, stream, ld=ldp) == 0
     torch.cuda.synchronize(dev)
     assert torch.cuda.mem_get_info(dev)[0] == free0
 
-    for out_ref, out_got in zip(ref, got):
-        for name, a, b in zip("STV", out_ref, out_got):
-            err = (a - b).abs().max().item()
-            assert err < TOL[name], (basis, name, err)
+    for name, a, b in zip("STV", ref[0], got0):
+        err = (a - b).abs().max().item()
+        assert err < TOL[name], (basis, name, err)
+    for name, a, b in zip("STV", ref[1], got1):
+        # column j of the column-major result is row j of the torch array; the matrices
+        # are symmetric, so the n x n block compares with either orientation
+        err = (a - b[:, :n]).abs().max().item()
+        assert err < TOL[name], (basis, name, err)
+        assert torch.isnan(b[:, n:]).all(), (basis, name, "padding rows written")
     ai.close()
 
 
-def test_no_alloc_rejects_too_many_charges():
+def test_no_alloc_rejects_bad_sizes_before_writing():
+    """More charges than the table holds, or a leading dimension below nbf: status
+    CQG_ERR_BAD_ARG with a message, and nothing written."""
     import torch
     from chronusq_public_b200.aointegrals import AOIntegrals
     mol = water_cluster(2, 4)
@@ -85,11 +103,17 @@ def test_no_alloc_rejects_too_many_charges():
     ai = AOIntegrals(bs)
     n = ai.nBasis
     dev = torch.device("cuda", 0)
-    out = [torch.zeros((n, n), dtype=torch.float64, device=dev) for _ in range(3)]
+    stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    out = [torch.full((n, n), 7.0, dtype=torch.float64, device=dev) for _ in range(3)]
     Z = np.ones(MAX_CHARGES + 1)
     R = np.zeros((MAX_CHARGES + 1, 3))
-    st = _no_alloc(ai, MAX_CHARGES + 1, Z.ctypes.data, R.ctypes.data, out,
-                   ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    st = _no_alloc(ai, MAX_CHARGES + 1, Z.ctypes.data, R.ctypes.data, out, stream)
     assert st == 1                                   # CQG_ERR_BAD_ARG
     assert b"4096" in ai._L.cqg_last_error(ai._ctx)
+    Zn, Rn = _charges(mol, 0, 0)
+    st = _no_alloc(ai, len(Zn), Zn.ctypes.data, Rn.ctypes.data, out, stream, ld=n - 1)
+    assert st == 1
+    assert b"leading dimension" in ai._L.cqg_last_error(ai._ctx)
+    torch.cuda.synchronize(dev)
+    assert all(bool((x == 7.0).all()) for x in out)
     ai.close()
