@@ -6,18 +6,28 @@ include/singleslater/singleslater_fock.h:31-93 -> newTwoEContractDirect) for a s
 (H2O)_32 cluster at liquid density in cc-pVDZ (768 basis functions, quartet classes up to
 (dd|dd)), Schwarz threshold 1e-14 (the reference default, include/aointegrals.h:334), on
 the SAD-guess density.  One step = one Fock build over one density.  Metric: screened
-unique shell quartets per second (the reference's loop unit, contract.h:96-131).  The line
-also carries the time to a converged SCF (|dE| <= 1 uEh) of the plain FP64 build and of
-the mixed-precision incremental build.
+unique shell quartets per second (the reference's loop unit, contract.h:96-131).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 The ``value`` leg times the device path (inputs resident in HBM, CUDA events on the
 launching stream, L2 flushed between steps).  ``e2e`` times the same build through the C
 ABI with host buffers (host->device and device->host copies inside the timed region).
+On one GPU the line also carries, untimed by the contract:
+
+* ``scf``: time to a converged SCF (|dE| <= 1 uEh) of (H2O)_32 cc-pVDZ for the plain FP64
+  build (median of repeats), the mixed-precision incremental build with the FP32 cutoff
+  swept 1e-10..1e-6, and the learned-guess arms, each with |dE| and max|dG| against FP64;
+* ``scf_headline``: the same arms on (H2O)_64 cc-pVDZ, with the speed-ups with and without
+  the relaxed mixed-phase screen;
+* ``batch_scf``: 512 clusters (H2O)_n, n in 1..24, 6-31G(d), batched (CUDA graph, one
+  launch per class and iteration) against one-at-a-time SCFs (stratified sample);
+* ``cpu_baseline``: the oracle on the host cores, one residue class of the outer loop.
+
 ``--impl reference`` times the CPU restatement of the reference loop (the oracle; the
-reference itself needs Libint and cannot be built here) on the host cores, on a bounded
-slice of the same workload.
+reference itself needs Libint and cannot be built here) on all host cores, with its input
+density computed on the host as well: the timed steps are residue classes of the outer
+shell index that together make up one whole Fock build.
 """
 from __future__ import annotations
 
@@ -58,15 +68,20 @@ def synthetic_density(bs, seed):
     return np.ascontiguousarray(D)
 
 
-def build_workload(name, density="sad"):
-    """Molecule, basis and the density of the benchmarked Fock build: the SAD-guess
-    density of the SCF (atomic UHF densities, one Fock build, diagonalised; computed on
-    the GPU) or, with density="synthetic", a seeded distance-decaying matrix."""
+def workload_geometry(name):
+    """Molecule and basis of a named workload (host-only: no GPU code is loaded)."""
     from chronusq_public_b200.basis import BasisSet
     from chronusq_public_b200.molecule import water_cluster, single_water
     w = WORKLOADS[name]
     mol = single_water(w["seed"]) if w["nwater"] == 1 else water_cluster(w["nwater"], w["seed"])
-    bs = BasisSet(w["basis"], mol.atoms, mol.coords)
+    return w, mol, BasisSet(w["basis"], mol.atoms, mol.coords)
+
+
+def build_workload(name, density="sad"):
+    """Molecule, basis and the density of the benchmarked Fock build: the SAD-guess
+    density of the SCF (atomic UHF densities, one Fock build, diagonalised; computed on
+    the GPU) or, with density="synthetic", a seeded distance-decaying matrix."""
+    w, mol, bs = workload_geometry(name)
     if density == "synthetic":
         D = synthetic_density(bs, 1234)
     else:
@@ -77,6 +92,27 @@ def build_workload(name, density="sad"):
         D = 0.5 * (D + D.T)
         hf.close()
     return w, mol, bs, D
+
+
+def reference_workload(name, density="sad"):
+    """The same workload built on the host alone for the reference arm: the SAD-guess
+    density comes from the oracle's restatement of SingleSlater::formGuess (atomic UHF
+    densities, one Fock build with the oracle's contraction, Loewdin diagonalisation), so
+    the arm never loads the GPU library."""
+    w, mol, bs = workload_geometry(name)
+    if density == "synthetic":
+        return w, mol, bs, synthetic_density(bs, 1234)
+    from oracle import scf_ref
+    return w, mol, bs, scf_ref.sad_guess_density(mol, bs, w["thresh"], nthreads=os.cpu_count())
+
+
+def gpu_library_loaded():
+    """Whether this process has mapped the engine's CUDA library (read from /proc)."""
+    try:
+        with open("/proc/self/maps") as f:
+            return any("libcqgpu" in line for line in f)
+    except OSError:
+        return None
 
 
 class ClockSampler:
@@ -145,71 +181,82 @@ def dist_setup():
     return ws, rank, local
 
 
+def oracle_build_part(ob, Q, D, thresh, modulus, residue, threads):
+    """One residue class of the oracle's Fock build (RHF formPT lists: COULOMB 1, EXCHANGE
+    -0.5): the quartets whose outermost shell index s1 satisfies s1 % modulus == residue.
+    The `modulus` classes together are the whole loop of contract.h:96-193.  Returns
+    (quartets, seconds)."""
+    from oracle import oracle as O
+    G = np.zeros_like(D, order="F")
+    t0 = time.perf_counter()
+    n = O.twoe_contract_direct(ob, [D, D], [G, G], [0, 1], [1.0, -0.5], thresh=thresh, Q=Q,
+                               nthreads=threads, s1_residue=(modulus, residue))
+    return n, time.perf_counter() - t0
+
+
+_PRIMES = (5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53, 59, 61)
+
+
 def cpu_baseline(bs, D, thresh, target_s=15.0, nthreads=0):
-    """Time the oracle (CPU restatement of the reference loop) on a bounded slice of the
-    same workload: all quartets whose largest shell index s1 lies in a window at the top
-    of the shell range, grown until the slice takes about `target_s` seconds."""
+    """Time the oracle (CPU restatement of the reference loop) on a bounded sample of the
+    same workload: one residue class of the outermost shell index (s1 % K == 1).  K is a
+    prime above 3, so that it shares no factor with the shells per molecule (12 for water
+    in cc-pVDZ): the class then holds every shell type of every part of the cluster in
+    equal measure.  K is chosen from a first class of 61 so that the sample takes about
+    `target_s` seconds."""
     from oracle import oracle as O
     ob = O.OracleBasis.from_basis(bs)
     Q = O.schwarz(ob)
     Dm = np.asfortranarray(D)
-    nsh = bs.nshell
-    width = 1
     threads = nthreads or os.cpu_count()
-    while True:
-        G = np.zeros_like(Dm, order="F")
-        t0 = time.perf_counter()
-        n = O.twoe_contract_direct(ob, [Dm, Dm], [G, G], [0, 1], [1.0, -0.5], thresh=thresh, Q=Q,
-                                   nthreads=threads, s1_range=(nsh - width, nsh))
-        dt = time.perf_counter() - t0
-        if dt >= target_s / 4 or width >= nsh:
-            scale = max(1, int(round(target_s / max(dt, 1e-3))))
-            if scale > 1 and width < nsh:
-                width = min(nsh, width * int(math.ceil(scale ** (1 / 3.0))))
-                G = np.zeros_like(Dm, order="F")
-                t0 = time.perf_counter()
-                n = O.twoe_contract_direct(ob, [Dm, Dm], [G, G], [0, 1], [1.0, -0.5], thresh=thresh, Q=Q,
-                                           nthreads=threads, s1_range=(nsh - width, nsh))
-                dt = time.perf_counter() - t0
-            return {"value": n / dt, "unit": "quartets/s", "cores": threads, "kind": "port",
-                    "sample": "oracle restatement of newTwoEContractDirect (FP64 Obara-Saika/HGP, OpenMP), "
-                              "quartets with s1 in [%d,%d) of %d shells: %d quartets in %.2f s"
-                              % (nsh - width, nsh, nsh, n, dt),
-                    "quartets": n, "seconds": dt}
-        width *= 2
+    n0, t0 = oracle_build_part(ob, Q, Dm, thresh, 61, 0, threads)
+    want = 61 * t0 / max(target_s, 1e-3)
+    K = min(_PRIMES, key=lambda p: abs(p - want))
+    n, dt = oracle_build_part(ob, Q, Dm, thresh, K, 1, threads)
+    return {"value": n / dt, "unit": "quartets/s", "cores": threads, "kind": "port",
+            "sample": "oracle restatement of newTwoEContractDirect (FP64 Obara-Saika/HGP, OpenMP), "
+                      "quartets with s1 %% %d == 1 (one of %d residue classes of the outermost shell index; "
+                      "%d is prime, so the class spans every shell type across the whole cluster): "
+                      "%d quartets in %.2f s" % (K, K, K, n, dt),
+            "quartets": n, "seconds": dt, "residue_classes": K}
 
 
 def run_reference(args, ws, rank):
+    """Reference arm: the CPU restatement of the reference loop (the reference needs Libint,
+    which cannot be built here), on all host cores, with no GPU code loaded.  The timed
+    steps split one full Fock build into `steps` residue classes of the outermost shell
+    index (step k: s1 % steps == k), so together they are exactly one whole build; the
+    warm-up steps run classes of 4 x steps."""
     if rank != 0:
         return
-    w, mol, bs, D = build_workload(args.workload, args.density)
-    base = cpu_baseline(bs, D, w["thresh"], target_s=args.ref_seconds)
     from oracle import oracle as O
+    w, mol, bs, D = reference_workload(args.workload, args.density)
     ob = O.OracleBasis.from_basis(bs)
     Q = O.schwarz(ob)
-    nsh = bs.nshell
-    width = int(base["sample"].split("[")[1].split(",")[0])
-    lo = width
-    times, counts = [], []
     Dm = np.asfortranarray(D)
-    for it in range(args.warmup + args.steps):
-        G = np.zeros_like(Dm, order="F")
-        t0 = time.perf_counter()
-        n = O.twoe_contract_direct(ob, [Dm, Dm], [G, G], [0, 1], [1.0, -0.5], thresh=w["thresh"], Q=Q,
-                                   nthreads=os.cpu_count(), s1_range=(lo, nsh))
-        dt = time.perf_counter() - t0
-        if it >= args.warmup:
-            times.append(dt)
-            counts.append(n)
+    threads = os.cpu_count()
+    K = max(1, args.steps)
+    for j in range(args.warmup):
+        oracle_build_part(ob, Q, Dm, w["thresh"], 4 * K, j % (4 * K), threads)
+    times, counts = [], []
+    for k in range(args.steps):
+        n, dt = oracle_build_part(ob, Q, Dm, w["thresh"], K, k, threads)
+        times.append(dt)
+        counts.append(n)
     v = sum(counts) / sum(times)
+    cfg = config_of(args, w, bs)
+    cfg["density"] = ("SAD guess density, computed on the host by the oracle's restatement of "
+                      "formGuess" if args.density == "sad" else cfg["density"])
     line = {"impl": "reference", "metric": "fock_build_quartets_per_s", "value": v, "unit": "quartets/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_of(args, w, bs),
-            "cpu_baseline": {"value": v, "unit": "quartets/s", "cores": os.cpu_count(), "kind": "port",
-                             "sample": "each step: oracle restatement (no Libint here) on quartets with s1 in "
-                                       "[%d,%d) of %d shells (%d quartets)" % (lo, nsh, nsh, counts[0])},
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "quartets_per_build": sum(counts), "seconds_per_build": sum(times),
+            "cpu_baseline": {"value": v, "unit": "quartets/s", "cores": threads, "kind": "port",
+                             "sample": "oracle restatement of newTwoEContractDirect (no Libint here); timed step "
+                                       "k runs the quartets with s1 %% %d == k, so the %d timed steps together "
+                                       "are one whole Fock build (%d quartets)" % (K, args.steps, sum(counts))},
+            "gpu_library_loaded": gpu_library_loaded(),
             "e2e": {"value": v, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -228,48 +275,88 @@ def config_of(args, w, bs):
 SCF_ARMS = ("plain", "mixed", "learned", "mixed_learned", "mixed_learned_context")
 
 
-def scf_compare(mol, bs, thresh, cutoff, sweep=(), autotune=True, arms=SCF_ARMS):
+def max_dG_vs_fp64(ints, densities, mixed, cutoff, threshold, base_thresh):
+    """max over `densities` of max|PT_arm[D] - PT_fp64[D]| (RHF formPT, 2J - K): the arm's
+    builds (FP32 below `cutoff` when `mixed`, screened at `threshold`) against the all-FP64
+    build at the context's threshold `base_thresh`.  The context is left in FP64 at
+    `base_thresh`."""
+    from chronusq_public_b200.aointegrals import PREC_FP64, PREC_MIXED
+    worst = 0.0
+    for D in densities:
+        ints.setPrecision(PREC_FP64, 0.0)
+        ints.thresholdSchwartz = base_thresh
+        ref, _ = ints.formPT(D)
+        if mixed:
+            ints.setPrecision(PREC_MIXED, cutoff)
+        ints.thresholdSchwartz = threshold
+        got, _ = ints.formPT(D)
+        worst = max(worst, float((got - ref).abs().max()))
+    ints.setPrecision(PREC_FP64, 0.0)
+    ints.thresholdSchwartz = base_thresh
+    return worst
+
+
+def scf_compare(mol, bs, thresh, cutoff, sweep=(), autotune=True, arms=SCF_ARMS, plain_repeats=1):
     """Time to converged SCF: plain FP64 GPU build vs mixed precision + incremental build,
     each with the SAD and the learned guess.  Times include the guess (atomic SCFs cached
-    beforehand) and every iteration.  `arms` picks a subset; without the plain arm, each
-    arm's time to 1 uEh is measured against its own converged energy (the final phase of
-    every arm is FP64 at the context's threshold), and the output says so."""
+    beforehand) and every iteration.  The plain arm runs `plain_repeats` times and its
+    median time to 1 uEh is the reference of the speed-ups (its DIIS path varies from run
+    to run).  Every arm reports |dE| against the FP64 energy and max|dG|: the largest
+    element of PT_arm[D] - PT_fp64[D] over the SAD-guess density and the converged FP64
+    density, with the arm's precision, FP32 cutoff and screening threshold.  `arms` picks a
+    subset; without the plain arm, each arm's time to 1 uEh is measured against its own
+    converged energy (the final phase of every arm is FP64 at the context's threshold)."""
+    import torch
     from chronusq_public_b200.scf import SingleSlater
     warm = SingleSlater(mol, bs, thresholdSchwartz=thresh)
     Pg, Pzg, _, _ = warm.formGuess()      # atomic SAD densities cached, kernels warm
     if autotune:
         warm.ints.autotune_next()         # launch shapes tuned on one full build, shared by every arm
         warm.formPT(Pg, Pzg)
-    out, E64 = {}, None
+    ints = warm.ints
+    out, E64, dens = {}, None, [Pg]
     if "plain" in arms:
-        plain = SingleSlater(mol, bs, ints=warm.ints)
-        E64 = plain.SCF3()
-        out["plain_fp64"] = {"energy": E64, "iterations": plain.nSCFIter, "seconds": plain.scf_seconds,
-                             "seconds_to_1uEh": plain.time_to(E64, 1e-6), "fock_builds": plain.fock_builds,
-                             "fock_seconds": plain.fock_seconds}
+        runs = []
+        for _ in range(max(1, plain_repeats)):
+            plain = SingleSlater(mol, bs, ints=ints)
+            E = plain.SCF3()
+            runs.append({"energy": E, "iterations": plain.nSCFIter, "seconds": plain.scf_seconds,
+                         "seconds_to_1uEh": plain.time_to(E, 1e-6), "fock_builds": plain.fock_builds,
+                         "fock_seconds": plain.fock_seconds})
+            if E64 is None:
+                E64 = E
+                dens.append(plain.onePDMScalar.clone())
+        t1 = [r["seconds_to_1uEh"] for r in runs]
+        out["plain_fp64"] = dict(runs[0])
+        out["plain_fp64"].update({"repeats": len(runs), "seconds_to_1uEh": statistics.median(t1),
+                                  "seconds_to_1uEh_each": t1, "energy_spread": max(r["energy"] for r in runs) -
+                                  min(r["energy"] for r in runs)})
     else:
         out["reference_energy"] = "each arm's own converged energy (no plain FP64 arm run)"
 
-    def record(hf, E, extra):
+    def record(hf, E, extra, mixed, c, mthr):
         ref = E if E64 is None else E64
         r = {"energy": E, "iterations": hf.nSCFIter, "seconds": hf.scf_seconds,
              "seconds_to_1uEh": hf.time_to(ref, 1e-6)}
         if E64 is not None:
             r["abs_dE_vs_fp64"] = abs(E - E64)
+        thr = thresh if (mthr is None or not mixed) else max(thresh, mthr)
+        r["max_abs_dG_vs_fp64"] = max_dG_vs_fp64(ints, dens, mixed, c, thr, thresh)
+        r["mixed_phase_threshold"] = thr if mixed else None
         r.update(extra)
         return r
 
     if "mixed" in arms:
         runs = {}
         for c in sorted(set([cutoff] + list(sweep))):
-            mx = SingleSlater(mol, bs, ints=warm.ints)
+            mx = SingleSlater(mol, bs, ints=ints)
             mx.precision, mx.fp32_cutoff, mx.incremental = "mixed", c, True
             E = mx.SCF3()
             runs["%.0e" % c] = record(mx, E, {"fp32_quartets": mx.fp32_quartets,
                                               "fp64_switch_iteration": mx.phase_switch_iter,
-                                              "mixed_phase_threshold": mx.mixed_threshold})
+                                              "fp32_cutoff": c}, True, c, mx.mixed_threshold)
+            runs["%.0e" % c]["max_abs_dG_fp32_only"] = max_dG_vs_fp64(ints, dens, True, c, thresh, thresh)
         out["mixed_incremental"] = runs["%.0e" % cutoff]
-        out["mixed_incremental"]["fp32_cutoff"] = cutoff
         if sweep:
             out["cutoff_sweep"] = runs
     # learned initial density (network trained on this engine's converged cluster densities)
@@ -288,20 +375,25 @@ def scf_compare(mol, bs, thresh, cutoff, sweep=(), autotune=True, arms=SCF_ARMS)
                                        True, None)):
             if arm not in arms:
                 continue
-            lg = SingleSlater(mol, bs, ints=warm.ints)
+            lg = SingleSlater(mol, bs, ints=ints)
             lg.guess, lg.guess_model, lg.guess_source_basis = "LEARNED", net, source
             if mixed:
                 lg.precision, lg.fp32_cutoff, lg.incremental, lg.mixed_threshold = "mixed", cutoff, True, mthr
             E = lg.SCF3()
             out[key] = record(lg, E, {"guess_used": lg.guess_used, "weights": os.path.basename(wpath),
-                                      "guess_projected_from": source})
+                                      "guess_projected_from": source}, mixed, cutoff, mthr)
     t_plain = out.get("plain_fp64", {}).get("seconds_to_1uEh")
-    for key, name in (("mixed_incremental", "speedup_time_to_1uEh"),
-                      ("mixed_incremental_learned", "speedup_time_to_1uEh_mixed_learned")):
+    for key, name in (("mixed_incremental", "speedup_time_to_1uEh_mixed"),
+                      ("learned_fp64", "speedup_time_to_1uEh_learned"),
+                      ("mixed_incremental_learned", "speedup_time_to_1uEh_mixed_learned"),
+                      ("mixed_incremental_learned_context_threshold",
+                       "speedup_time_to_1uEh_mixed_learned_without_relaxed_screen")):
         t = out.get(key, {}).get("seconds_to_1uEh")
         if t_plain and t:
             out[name] = t_plain / t
+    out["speedup_reference"] = "median of the plain FP64 arm's repeats"
     warm.close()
+    torch.cuda.synchronize()
     return out
 
 
@@ -318,14 +410,18 @@ def main():
     ap.add_argument("--density", default="sad", choices=["sad", "synthetic"])
     ap.add_argument("--no-scf", action="store_true", help="skip the time-to-converged-SCF comparison")
     ap.add_argument("--fp32-cutoff", type=float, default=1e-8)
-    ap.add_argument("--sweep", action="store_true", help="also sweep the FP32 cutoff 1e-10..1e-6")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the FP32 cutoff sweep 1e-10..1e-6")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes instead of autotuned ones")
     ap.add_argument("--scf-arms", default=",".join(SCF_ARMS),
                     help="comma-separated SCF arms to run (%s)" % ", ".join(SCF_ARMS))
-    ap.add_argument("--batch", type=int, default=0,
-                    help="also run the batched-SCF comparison on this many (H2O)_n, n in 1..24, 6-31G(d)")
-    ap.add_argument("--batch-single", type=int, default=64, help="molecules converged one at a time")
+    ap.add_argument("--plain-repeats", type=int, default=3, help="runs of the plain FP64 SCF arm (median)")
+    ap.add_argument("--headline", default="h2o64-ccpvdz", choices=sorted(WORKLOADS) + ["none"],
+                    help="workload of the headline SCF comparison (all arms), 'none' to skip")
+    ap.add_argument("--batch", type=int, default=512,
+                    help="molecules of the batched-SCF comparison ((H2O)_n, n in 1..24, 6-31G(d)); 0 skips it")
+    ap.add_argument("--batch-per-size", type=int, default=2,
+                    help="molecules per cluster size converged one at a time (stratified sample)")
     args = ap.parse_args()
     bad = [a for a in args.scf_arms.split(",") if a not in SCF_ARMS]
     if bad:
@@ -435,14 +531,23 @@ def main():
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
-        if not args.no_scf:
+        extras = ws == 1                   # replicas (N > 1) report the Fock-build line only
+        if extras and not args.no_scf:
             line["scf"] = scf_compare(mol, bs, w["thresh"], args.fp32_cutoff,
-                                      sweep=(1e-10, 1e-9, 1e-8, 1e-7, 1e-6) if args.sweep else (),
-                                      autotune=not args.no_autotune, arms=args.scf_arms.split(","))
-        if args.batch > 0:
+                                      sweep=() if args.no_sweep else (1e-10, 1e-9, 1e-8, 1e-7, 1e-6),
+                                      autotune=not args.no_autotune, arms=args.scf_arms.split(","),
+                                      plain_repeats=args.plain_repeats)
+            if args.headline != "none" and args.headline != args.workload:
+                hw, hmol, hbs = workload_geometry(args.headline)
+                line["scf_headline"] = {"workload": args.headline, "nbasis": hbs.nbasis}
+                line["scf_headline"].update(scf_compare(hmol, hbs, hw["thresh"], args.fp32_cutoff,
+                                                        autotune=not args.no_autotune,
+                                                        arms=args.scf_arms.split(","),
+                                                        plain_repeats=args.plain_repeats))
+        if extras and args.batch > 0:
             from chronusq_public_b200.workloads import batch_scf_comparison
-            line["batch_scf"] = batch_scf_comparison(args.batch, args.batch_single)
-        if not args.no_cpu_baseline and ws == 1:
+            line["batch_scf"] = batch_scf_comparison(args.batch, args.batch_per_size)
+        if extras and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(bs, D, w["thresh"], target_s=args.ref_seconds)
         print(json.dumps(line), flush=True)
         if args.class_table:

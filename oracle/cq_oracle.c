@@ -425,13 +425,15 @@ void oracle_shblk_norm(int nshell, const int *L, const int *pure, const double *
  * exactly as contract.h:107 does.  If `per_class` is non-NULL it receives the screened
  * quartet count per (la,lb,lc,ld) in shell-index orientation, indexed
  * ((la*5+lb)*5+lc)*5+ld.  s1_begin/s1_end (-1 = all) restrict the outermost shell index,
- * which the benchmark uses to time a bounded slice of a large workload. */
+ * and s1_mod > 1 keeps only s1 with s1 % s1_mod == s1_rem: the benchmark times a large
+ * workload as s1_mod such residue classes, which together make up the whole loop. */
 long long oracle_twoe_contract_direct(int nshell, const int *L, const int *pure, const int *nprim,
                                       const double *alpha, const double *coef, const double *centers,
                                       const double *const *sph, const double *Q, double thresh,
                                       int nmat, const double *const *X, double *const *AX,
                                       const int *types, const double *scale, int ld, int nthreads,
-                                      long long *per_class, int s1_begin, int s1_end) {
+                                      long long *per_class, int s1_begin, int s1_end, int s1_mod,
+                                      int s1_rem) {
   obasis B; obasis_init(&B, nshell, L, pure, nprim, alpha, coef, centers, sph);
   size_t nbf = B.nbf;
   double **blk = (double **)malloc(sizeof(double *) * nmat);
@@ -462,7 +464,8 @@ long long oracle_twoe_contract_direct(int nshell, const int *L, const int *pure,
     if (s1_begin < 0) s1_begin = 0;
     for (int s1 = 0; s1 < nshell; s1++) {
       size_t bf1_s = B.bfoff[s1]; int n1 = B.size[s1];
-      if (s1 < s1_begin || s1 >= s1_end) {  /* bounded sample: keep the global counter */
+      if (s1 < s1_begin || s1 >= s1_end || (s1_mod > 1 && s1 % s1_mod != s1_rem)) {
+        /* bounded sample: skip this s1 but keep the global counter */
         unsigned long m = (unsigned long)s1;
         s1234 += (m + 1) * (m * (m + 1) / 2) + (m + 1) * (m + 2) / 2;
         continue;

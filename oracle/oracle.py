@@ -53,7 +53,7 @@ def lib():
         _lib.oracle_twoe_contract_direct.argtypes = [
             ctypes.c_int, i, i, i, d, d, d, pp, d, ctypes.c_double,
             ctypes.c_int, pp, pp, i, d, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong),
-            ctypes.c_int, ctypes.c_int]
+            ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         _lib.oracle_twoe_contract_direct.restype = ctypes.c_longlong
         _lib.oracle_one_e.argtypes = [ctypes.c_int, i, i, i, d, d, d, pp, ctypes.c_int, d, d, d, d, d]
         _lib.oracle_dipole.argtypes = [ctypes.c_int, i, i, i, d, d, d, pp, d, d, d, d]
@@ -188,9 +188,11 @@ def shblk_norm(ob: OracleBasis, X: np.ndarray) -> np.ndarray:
 def twoe_contract_direct(ob: OracleBasis, X: Sequence[np.ndarray], AX: List[np.ndarray],
                          types: Sequence[int], scale: Sequence[float], thresh: float = 1e-14,
                          Q: np.ndarray = None, nthreads: int = 0, per_class: bool = False,
-                         s1_range=(-1, -1)):
+                         s1_range=(-1, -1), s1_residue=(1, 0)):
     """AX[i] += 0.5*scale[i]*G_i (in place, Fortran-ordered arrays).  Returns the number of
-    screened quartets (and the per-(la,lb,lc,ld) histogram when ``per_class``)."""
+    screened quartets (and the per-(la,lb,lc,ld) histogram when ``per_class``).
+    ``s1_range`` restricts the outermost shell index to [lo, hi); ``s1_residue = (m, r)``
+    keeps only s1 with s1 % m == r (the m residue classes partition the loop)."""
     if Q is None:
         Q = schwarz(ob)
     Q = np.asfortranarray(Q)
@@ -209,7 +211,7 @@ def twoe_contract_direct(ob: OracleBasis, X: Sequence[np.ndarray], AX: List[np.n
         ctypes.cast(xp, ctypes.POINTER(ctypes.c_void_p)), ctypes.cast(ap, ctypes.POINTER(ctypes.c_void_p)),
         t.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(s), Xs[0].shape[0], int(nthreads),
         hist.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)) if per_class else None,
-        int(s1_range[0]), int(s1_range[1]))
+        int(s1_range[0]), int(s1_range[1]), int(s1_residue[0]), int(s1_residue[1]))
     if per_class:
         return int(n), hist.reshape(5, 5, 5, 5)
     return int(n)
