@@ -110,3 +110,94 @@ def test_integration_shim_compiles_links_and_runs(tmp_path):
         assert abs(float(out.split()[1]) - 2 * 1.1283791670955126) < 1e-12, out
     else:
         assert out == "error: cqg_create failed", out
+
+
+# Reads the basis and a density from a text file, calls the shim's newTwoEContractDirect
+# with the RHF formPT lists (COULOMB 1.0, EXCHANGE -0.5 on the same X and AX) and writes AX.
+MAIN_FILE = r"""
+#include <fstream>
+int main(int argc, char **argv) {
+  using namespace ChronusQ;
+  std::ifstream in(argv[1]);
+  int nsh = 0, nbf = 0;
+  in >> nsh >> nbf;
+  BasisSet bs;
+  for (int s = 0; s < nsh; s++) {
+    int l, pure, np;
+    in >> l >> pure >> np;
+    libint2::Shell sh;
+    sh.alpha.resize(np);
+    sh.contr.push_back({l, pure != 0, std::vector<double>(np)});
+    for (int k = 0; k < np; k++) in >> sh.alpha[k];
+    for (int k = 0; k < np; k++) in >> sh.contr[0].coeff[k];
+    for (int k = 0; k < 3; k++) in >> sh.O[k];
+    bs.shells_.push_back(sh);
+  }
+  RealMatrix X{std::vector<double>((size_t)nbf * nbf)}, AX{std::vector<double>((size_t)nbf * nbf, 0.0)};
+  for (auto &v : X.v) in >> v;          // column-major
+  AOIntegrals ints;
+  ints.basisSet_ = &bs;
+  ints.nBasis_ = nbf;
+  ints.thresholdSchwartz_ = 1e-12;
+  std::vector<std::reference_wrapper<RealMatrix>> xs{X, X}, axs{AX, AX};
+  std::vector<AOIntegrals::ERI_CONTRACTION_TYPE> types{AOIntegrals::COULOMB, AOIntegrals::EXCHANGE};
+  std::vector<double> scale{1.0, -0.5};
+  try {
+    ints.newTwoEContractDirect(xs, axs, types, scale);
+  } catch (const std::exception &e) {
+    std::cout << "error: " << e.what() << "\n";
+    return 1;
+  }
+  std::ofstream out(argv[2]);
+  out.precision(17);
+  for (double v : AX.v) out << v << "\n";
+  return 0;
+}
+"""
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(shutil.which("g++") is None, reason="no C++ compiler")
+def test_integration_shim_water_631gd_matches_oracle(tmp_path):
+    """The maintainer's C++ body, linked to libcqgpu.so, on a seeded water in 6-31G(d) with
+    a random symmetric density: AX = 2J[X] - K[X] within 1e-10 of the oracle's
+    newTwoEContractDirect restatement (include/aointegrals.h:474-480)."""
+    import numpy as np
+    from chronusq_public_b200.basis import BasisSet
+    from chronusq_public_b200.molecule import single_water
+    from oracle import oracle as O
+
+    lib = os.path.join(LIBDIR, "libcqgpu.so")
+    assert os.path.exists(lib), "libcqgpu.so not built"
+    mol = single_water(0)
+    bs = BasisSet("6-31g*", mol.atoms, mol.coords)
+    L, pure, nprim, alpha, coef, centers = bs.flat()
+    n = bs.nbasis
+    rng = np.random.default_rng(21)
+    a = rng.uniform(-1, 1, (n, n))
+    X = np.asfortranarray(0.5 * (a + a.T))
+    lines = ["%d %d" % (len(L), n)]
+    p = 0
+    for s in range(len(L)):
+        k = int(nprim[s])
+        lines.append("%d %d %d" % (L[s], pure[s], k))
+        lines.append(" ".join(repr(float(x)) for x in alpha[p:p + k]))
+        lines.append(" ".join(repr(float(x)) for x in coef[p:p + k]))
+        lines.append(" ".join(repr(float(x)) for x in centers[s]))
+        p += k
+    lines.append(" ".join(repr(float(x)) for x in X.ravel(order="F")))
+    (tmp_path / "in.txt").write_text("\n".join(lines) + "\n")
+    src = tmp_path / "shim.cpp"
+    src.write_text(PRELUDE + _shim_source() + MAIN_FILE)
+    exe = tmp_path / "shim"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Werror=return-type", str(src), "-o", str(exe),
+                    "-I", os.path.join(ROOT, "include"), "-L", LIBDIR, "-lcqgpu", "-Wl,-rpath," + LIBDIR],
+                   check=True, capture_output=True, text=True)
+    r = subprocess.run([str(exe), str(tmp_path / "in.txt"), str(tmp_path / "out.txt")],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    AX = np.loadtxt(tmp_path / "out.txt").reshape((n, n), order="F")
+    ob = O.OracleBasis.from_basis(bs)
+    ref = np.zeros((n, n), order="F")
+    O.twoe_contract_direct(ob, [X, X], [ref, ref], [O.COULOMB, O.EXCHANGE], [1.0, -0.5], thresh=1e-12)
+    assert np.abs(AX - ref).max() <= 1e-10
