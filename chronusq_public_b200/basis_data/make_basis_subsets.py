@@ -7,7 +7,7 @@ that the package parser reads them exactly as the reference reads the originals.
 
 Usage (run once, from the repository root, where the reference is mounted):
 
-    python chronusq_public_b200/basis_data/make_basis_subsets.py /root/reference/basis
+    python chronusq_public_b200/basis_data/make_basis_subsets.py <reference>/basis
 
 The records are copied verbatim (exponents and coefficients are published basis-set
 data: Pople 1969/1973, Dunning 1989).  Header comment lines are replaced by a one-line

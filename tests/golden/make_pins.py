@@ -6,7 +6,7 @@ matching inputs tests/testNNNN_serial_direct.inp (geometry, charge, multiplicity
 reference type and basis).  Only the Hartree-Fock rows the two-electron path drives
 (water RHF, Li and O2 UHF) are kept.
 
-    python tests/golden/make_pins.py /root/reference/oldTests.tgz
+    python tests/golden/make_pins.py <reference>/oldTests.tgz
 """
 import json
 import os
