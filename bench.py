@@ -261,6 +261,20 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def schedule_summary(ints, st):
+    """The autotuned schedule of the lists that had work: per class, the kernel form, CTAs
+    per SM, warps per CTA and quartets claimed per warp."""
+    sch = ints.schedule()
+    out = {}
+    for k, (name, nq) in enumerate(st["class_quartets"].items()):
+        if nq <= 0:
+            continue
+        out[name] = {"form": "warp" if sch["warp_form"][k] else "thread", "cta_per_sm": sch["cta_per_sm"][k],
+                     "warps_per_cta": sch["warps_per_cta"][k], "quartets_per_warp": sch["quartets_per_warp"][k],
+                     "ms": round(st["class_ms"][name], 4)}
+    return out
+
+
 def config_of(args, w, bs):
     return {"workload": args.workload, "molecule": "(H2O)_%d" % w["nwater"], "basis": w["basis"],
             "nbasis": bs.nbasis, "nshell": bs.nshell, "schwarz_threshold": w["thresh"],
@@ -269,7 +283,8 @@ def config_of(args, w, bs):
             "geometry": "seeded water cluster at 1.0 g/cm^3 (Poisson-disk O centres, min O-O 2.6 A)",
             "l2": "flushed between steps (256 MiB write)",
             "precision": "fp64", "parallelism": "replicas" if args.gpus > 1 else "single",
-            "launch_shapes": "default" if args.no_autotune else "autotuned in the first warm-up build"}
+            "launch_shapes": ("from %s" % os.path.basename(args.schedule_in) if getattr(args, "schedule_in", None)
+                              else "default" if args.no_autotune else "autotuned in the first warm-up build")}
 
 
 SCF_ARMS = ("plain", "mixed", "learned", "mixed_learned", "mixed_learned_context")
@@ -413,6 +428,9 @@ def main():
     ap.add_argument("--no-sweep", action="store_true", help="skip the FP32 cutoff sweep 1e-10..1e-6")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes instead of autotuned ones")
+    ap.add_argument("--schedule-out", default=None, help="write the autotuned per-list schedule to this JSON file")
+    ap.add_argument("--schedule-in", default=None,
+                    help="use the per-list schedule in this JSON file (from --schedule-out) instead of autotuning")
     ap.add_argument("--scf-arms", default=",".join(SCF_ARMS),
                     help="comma-separated SCF arms to run (%s)" % ", ".join(SCF_ARMS))
     ap.add_argument("--plain-repeats", type=int, default=3, help="runs of the plain FP64 SCF arm (median)")
@@ -449,11 +467,16 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
 
-    if not args.no_autotune:
+    if args.schedule_in:
+        ints.setSchedule(**json.load(open(args.schedule_in)))
+    elif not args.no_autotune:
         ints.autotune_next()              # the first warm-up build picks every class's launch shape
     for _ in range(args.warmup):
         ints.formPT(Dd, PTs=PT)
     torch.cuda.synchronize()
+    if args.schedule_out and rank == 0:
+        with open(args.schedule_out, "w") as f:
+            json.dump(ints.schedule(), f)
     ints.setTiming(True)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     step_ms, eri_ms, quartets, mflops, launches, class_ms = [], [], [], [], 0, {}
@@ -530,6 +553,7 @@ def main():
                          "traffic": traffic},
             "gpu_launches": launches,
             "clocks": clk.summary(),
+            "schedule": schedule_summary(ints, st_last),
         }
         extras = ws == 1                   # replicas (N > 1) report the Fock-build line only
         if extras and not args.no_scf:
@@ -544,6 +568,9 @@ def main():
                                                         autotune=not args.no_autotune,
                                                         arms=args.scf_arms.split(","),
                                                         plain_repeats=args.plain_repeats))
+        if extras and not args.no_scf:
+            from chronusq_public_b200.learned_guess import training_throughput
+            line["guess_training"] = training_throughput(epochs=2)
         if extras and args.batch > 0:
             from chronusq_public_b200.workloads import batch_scf_comparison
             line["batch_scf"] = batch_scf_comparison(args.batch, args.batch_per_size)

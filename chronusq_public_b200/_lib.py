@@ -33,7 +33,7 @@ EXPORTED = [
     "cqg_set_basis_batch", "cqg_get_batch_layout", "cqg_twoe_contract_direct_batch", "cqg_one_e_batch",
     "cqg_set_graph_mode", "cqg_graph_status", "cqg_autotune_next", "cqg_get_launch_shapes", "cqg_set_active",
     "cqg_mlp_gemm_bf16", "cqg_mlp_silu_bwd", "cqg_mlp_to_bf16", "cqg_mlp_colsum", "cqg_mlp_mse", "cqg_mlp_adam",
-    "cqg_one_e_noalloc", "cqg_dipole",
+    "cqg_one_e_noalloc", "cqg_dipole", "cqg_get_schedule", "cqg_set_schedule",
 ]
 
 
@@ -90,6 +90,8 @@ def load(path: str = LIB_PATH):
     L.cqg_graph_status.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), i, i, i]
     L.cqg_autotune_next.argtypes = [vp]
     L.cqg_get_launch_shapes.argtypes = [vp, i, i]
+    L.cqg_get_schedule.argtypes = [vp, i, i, i, i]
+    L.cqg_set_schedule.argtypes = [vp, i, i, i, i]
     L.cqg_set_active.argtypes = [vp, ctypes.c_char_p]
     ll, f, fp = ctypes.c_longlong, ctypes.c_float, ctypes.POINTER(ctypes.c_float)
     L.cqg_mlp_gemm_bf16.argtypes = [vp, ll, ll, vp, ll, ll, vp, ll, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp,
@@ -112,7 +114,7 @@ def load(path: str = LIB_PATH):
                  "cqg_twoe_contract_direct_batch", "cqg_one_e_batch", "cqg_set_graph_mode",
                  "cqg_graph_status", "cqg_autotune_next", "cqg_get_launch_shapes", "cqg_set_active",
                  "cqg_mlp_gemm_bf16", "cqg_mlp_silu_bwd", "cqg_mlp_to_bf16", "cqg_mlp_colsum", "cqg_mlp_mse",
-                 "cqg_mlp_adam", "cqg_one_e_noalloc", "cqg_dipole"]:
+                 "cqg_mlp_adam", "cqg_one_e_noalloc", "cqg_dipole", "cqg_get_schedule", "cqg_set_schedule"]:
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

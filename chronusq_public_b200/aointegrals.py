@@ -125,10 +125,29 @@ class AOIntegrals:
 
     def launch_shapes(self):
         """(CTAs per SM, warps per CTA) chosen per class work list (0 = default)."""
-        cta = (ctypes.c_int * 110)()
-        wpb = (ctypes.c_int * 110)()
-        _lib.check(self._L.cqg_get_launch_shapes(self._ctx, cta, wpb), self._ctx)
-        return list(cta), list(wpb)
+        sch = self.schedule()
+        return sch["cta_per_sm"], sch["warps_per_cta"]
+
+    def schedule(self):
+        """Per class work list (FP64 lists then FP32 lists, 110 entries each): CTAs per SM,
+        warps per CTA and quartets claimed per warp (0 = default), and the kernel form
+        (1 = warp-cooperative, 0 = one quartet per thread)."""
+        out = [(ctypes.c_int * 110)() for _ in range(4)]
+        _lib.check(self._L.cqg_get_schedule(self._ctx, *out), self._ctx)
+        return {k: list(v) for k, v in zip(("cta_per_sm", "warps_per_cta", "quartets_per_warp", "warp_form"), out)}
+
+    def setSchedule(self, cta_per_sm=None, warps_per_cta=None, quartets_per_warp=None, warp_form=None):
+        """Set the per-list schedule (sequences of 110 ints as :meth:`schedule` returns them,
+        or one int for every list; None leaves that part unchanged)."""
+        def arr(v):
+            if v is None:
+                return None
+            v = [int(v)] * 110 if isinstance(v, (int, np.integer)) else [int(x) for x in v]
+            if len(v) != 110:
+                raise ValueError("a schedule has 110 entries (55 FP64 lists, 55 FP32 lists)")
+            return (ctypes.c_int * 110)(*v)
+        _lib.check(self._L.cqg_set_schedule(self._ctx, arr(cta_per_sm), arr(warps_per_cta), arr(quartets_per_warp),
+                                            arr(warp_form)), self._ctx)
 
     # ------------------------------------------------------------------ queries ---
     def computeSchwartz(self) -> np.ndarray:

@@ -188,13 +188,28 @@ cqg_status cqg_graph_status(cqg_ctx *ctx, long long *quartets, int *overflow, in
                             int *asymmetric);
 /* Autotuner: the next (non-graph, single-chunk) contraction times every candidate launch
  * shape of each class work list (persistent CTAs per SM; warps per CTA for the
- * warp-cooperative classes) and keeps the fastest for later calls.  The shapes are read
+ * warp-cooperative classes; quartets claimed per warp from the list's work queue) and keeps
+ * the fastest for later calls.  The shapes are read
  * back with cqg_get_launch_shapes (2 x 55 entries: FP64 lists then FP32 lists; 0 = default). */
 cqg_status cqg_autotune_next(cqg_ctx *ctx);
 /* Set which molecules of a batch take part in the following contractions (NULL: all);
  * a synchronous copy, to be called outside any captured region. */
 cqg_status cqg_set_active(cqg_ctx *ctx, const unsigned char *active);
 cqg_status cqg_get_launch_shapes(cqg_ctx *ctx, int *cta_per_sm, int *warps_per_cta);
+/* The same plus, per list, the work-queue chunk (the quartets one warp claims at a time:
+ * per-thread kernels in units of 32, one per lane; warp-cooperative kernels one after the
+ * other) and the kernel form (1 = warp-cooperative, 0 = one quartet per thread; classes
+ * that have both forms get theirs from the autotuner).  Any output may be NULL; 0 in the
+ * first three = default. */
+cqg_status cqg_get_schedule(cqg_ctx *ctx, int *cta_per_sm, int *warps_per_cta, int *quartets_per_warp,
+                            int *warp_form);
+/* Set the schedule of every list from arrays laid out as cqg_get_schedule's (NULL leaves
+ * that part unchanged; the kernel form is taken only for classes that have both forms):
+ * a schedule tuned once can be given to other contexts of the same system.  Entries out of
+ * range (CTAs per SM above 64, warps per CTA above 4, quartets per warp above 1024, a form
+ * other than 0 or 1) give CQG_ERR_BAD_ARG and change nothing. */
+cqg_status cqg_set_schedule(cqg_ctx *ctx, const int *cta_per_sm, const int *warps_per_cta,
+                            const int *quartets_per_warp, const int *warp_form);
 
 /* Statistics of the last contraction (synchronises the context's stream). */
 cqg_status cqg_get_stats(cqg_ctx *ctx, cqg_stats *out);

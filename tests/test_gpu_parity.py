@@ -208,3 +208,40 @@ def test_form_pt_rejects_short_leading_dimension_before_writing():
     assert b"leading dimension" in ints._L.cqg_last_error(ints._ctx)
     assert (PT == 7.0).all()                          # PT not zeroed on the rejected call
     ints.close()
+
+
+@pytest.mark.parametrize("basis,nwater,seed", [("cc-pvdz", 3, 11), ("cc-pvtz", 2, 17)])
+@pytest.mark.parametrize("form,qpw", [(1, 4), (0, 8)])
+def test_forced_schedule_matches_oracle(basis, nwater, seed, form, qpw):
+    """Every list run with a forced schedule -- the warp-cooperative form for the classes
+    that have both forms (or the per-thread form), and several quartets claimed per warp
+    from the work queue -- gives the oracle's G and quartet count (UHF lists)."""
+    mol = water_cluster(nwater, seed)
+    bs = BasisSet(basis, mol.atoms, mol.coords)
+    ob = O.OracleBasis.from_basis(bs)
+    Ps = rand_sym(bs.nbasis, 41)
+    Pz = rand_sym(bs.nbasis, 42, 0.2)
+    ints = _aoi()(bs)
+    ints.setSchedule(cta_per_sm=8, warps_per_cta=2, quartets_per_warp=qpw, warp_form=form)
+    sch = ints.schedule()
+    assert set(sch["quartets_per_warp"]) == {qpw}
+    PTs, PTz = ints.formPT(Ps, Pz)
+    st = ints.stats()
+    PTs_r, PTz_r, nr = O.form_pt(ob, Ps, Pz)
+    assert st["quartets"] == nr
+    assert np.abs(PTs - PTs_r).max() <= TOL_G
+    assert np.abs(PTz - PTz_r).max() <= TOL_G
+    ints.close()
+
+
+def test_set_schedule_rejects_out_of_range_entries():
+    from chronusq_public_b200._lib import CqgError
+    mol = single_water(4)
+    bs = BasisSet("6-31g*", mol.atoms, mol.coords)
+    ints = _aoi()(bs)
+    before = ints.schedule()
+    with pytest.raises(CqgError) as e:
+        ints.setSchedule(cta_per_sm=8, warp_form=2)
+    assert e.value.status == 1
+    assert ints.schedule() == before
+    ints.close()
