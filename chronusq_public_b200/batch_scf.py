@@ -109,10 +109,13 @@ class BatchSCF:
         density and the per-molecule flag of a usable prediction."""
         from .guess_model import predict_densities
         t = self.torch
+        t0 = time.perf_counter()
         P = self.B.zeros()
         preds = predict_densities(model, self.mols, self.bss)
         for m, Pm in enumerate(preds):
             self.B.view(P, m).copy_(t.as_tensor(Pm, dtype=t.float64, device=self.dev))
+        t.cuda.synchronize(self.dev)
+        self.predict_seconds = time.perf_counter() - t0
         ok = np.zeros(self.nmol, dtype=bool)
         sad = None
         for g in self.groups:
@@ -137,8 +140,11 @@ class BatchSCF:
         The guess density is the SAD superposition, or `density` (packed), or the one
         `model` (guess_model.PairMLP) predicts, made inside the timed region.
         use_graph: the batched Fock build of every iteration is one CUDA-graph replay
-        (captured once, after the guess build).  autotune: the guess build also picks the
-        launch shape of every class work list."""
+        (captured once, after the first iteration's build).  autotune: the first build from
+        a full (not block-diagonal) density picks the launch shape of every class work list:
+        the first iteration's build after a SAD guess, the guess build itself for a learned
+        or given density, so both guesses tune on the same kind of work lists.
+        `guess_seconds` records the time until the first iterate exists."""
         t = self.torch
         t.cuda.synchronize(self.dev)
         t0 = time.perf_counter()
@@ -146,14 +152,16 @@ class BatchSCF:
         # first iterate itself, and its build is the first iteration's
         first_PT = None
         self.guess_fallbacks = 0
+        sad = model is None and density is None
         if model is not None:
             P, ok = self.learned_density(model)
             self.guess_fallbacks = int((~ok).sum())
         else:
             P = self.sad_density() if density is None else density.clone()
-        if autotune:
+        if autotune and not sad:
             self.B.autotune_next()
         PT = self.B.formPT(P)
+        tune_first_iteration = autotune and sad
         graph = None
         self.graph_replays = 0
         self.graph_captures = 0
@@ -170,6 +178,8 @@ class BatchSCF:
             for g in self.groups:
                 F = 2.0 * g["H"] + self.gather(PT, g)
                 self.scatter(self._density(g["X"].transpose(-1, -2) @ F @ g["X"], g), g, P)
+        t.cuda.synchronize(self.dev)
+        self.guess_seconds = time.perf_counter() - t0
         active = np.ones(self.nmol, dtype=bool)
         Eold = t.zeros(self.nmol, dtype=t.float64, device=self.dev)
         energies = t.zeros(self.nmol, dtype=t.float64, device=self.dev)
@@ -186,7 +196,9 @@ class BatchSCF:
             tf = time.perf_counter()
             if first_PT is not None:
                 PT, first_PT = first_PT, None
-            elif use_graph and it == 0:
+            elif it == 0 and (use_graph or tune_first_iteration):
+                if tune_first_iteration:
+                    self.B.autotune_next()
                 PT = self.B.formPT(P, active=active.tolist())
             elif graph is not None:
                 self.B.set_active(active.tolist())

@@ -2,9 +2,10 @@
 // GPU with BF16 operands and FP32 accumulation.
 //
 //   k_gemm_bf16 : C[m][n] (+)= sum_k A(m,k) B(n,k), A and B BF16 with arbitrary strides
-//                 (transposes are strides), FP32 accumulation in registers over 64x64
-//                 tiles staged through shared memory; optional fused epilogue
-//                 Z = C + bias (FP32) and Y = SiLU(Z) (BF16).
+//                 (transposes are strides), on the tensor cores: mma.sync m16n8k16 BF16 x
+//                 BF16 -> FP32 over 128 x 128 x 32 block tiles staged in shared memory
+//                 (8 warps, 32 x 64 each); optional fused epilogue Z = C + bias (FP32) and
+//                 Y = SiLU(Z) (BF16).
 //   k_silu_bwd  : dZ = dY * SiLU'(Z)  (BF16 out, the next GEMM's operand)
 //   k_colsum    : db[n] = sum_m dZ[m][n]
 //   k_mse       : masked squared error, its gradient, and the loss sum
@@ -18,7 +19,7 @@
 
 namespace {
 
-constexpr int TM = 64, TN = 64, TK = 16;
+constexpr int GM = 128, GN = 128, GK = 32, GKP = GK + 8;   // block tile; padded smem rows
 
 __device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
 __device__ __forceinline__ float silu_grad(float z) {
@@ -26,59 +27,126 @@ __device__ __forceinline__ float silu_grad(float z) {
   return s * (1.0f + z * (1.0f - s));
 }
 
-// 256 threads, each computes a 4x4 sub-tile of the 64x64 output tile.
+// D += A B for one 16 x 8 x 16 tile (A row-major 16 x 16, B column-major 16 x 8, BF16
+// operands, FP32 accumulators).  Fragments (g = lane / 4, t = lane % 4):
+//   a[0] = A[g][2t..2t+1], a[1] = A[g+8][2t..], a[2] = A[g][2t+8..], a[3] = A[g+8][2t+8..]
+//   b[0] = B[2t..2t+1][g], b[1] = B[2t+8..2t+9][g]
+//   d[0..1] = D[g][2t..2t+1], d[2..3] = D[g+8][2t..2t+1]
+__device__ __forceinline__ void mma_16816(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// Stage rows [r0, r0 + 128) x k [k0, k0 + 32) of X(r, k) = X[r * sr + k * sk] into S[row][k]
+// (zero outside nrows x K).  Rows or k contiguous and 16-byte aligned: 8-element vector
+// loads; anything else element by element.
+__device__ __forceinline__ void stage_tile(const __nv_bfloat16 *__restrict__ X, long long sr, long long sk, int r0,
+                                           int nrows, int k0, int K, bool vec_k, bool vec_r,
+                                           __nv_bfloat16 (*S)[GKP]) {
+  const int tid = threadIdx.x;
+  const __nv_bfloat16 zero = __float2bfloat16(0.f);
+  if (vec_k) {                 // sk == 1, sr % 8 == 0, K % 8 == 0, X 16-byte aligned
+    for (int e = tid; e < 128 * (GK / 8); e += 256) {
+      const int rr = e / (GK / 8), kv = (e % (GK / 8)) * 8;
+      const int r = r0 + rr, k = k0 + kv;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (r < nrows && k < K) v = *reinterpret_cast<const uint4 *>(X + (long long)r * sr + k);
+      *reinterpret_cast<uint4 *>(&S[rr][kv]) = v;
+    }
+  } else if (vec_r) {          // sr == 1, sk % 8 == 0, nrows % 8 == 0, X 16-byte aligned
+    for (int e = tid; e < GK * 16; e += 256) {
+      const int kk = e / 16, rv = (e % 16) * 8;
+      const int r = r0 + rv, k = k0 + kk;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (r < nrows && k < K) v = *reinterpret_cast<const uint4 *>(X + r + (long long)k * sk);
+      const __nv_bfloat16 *h = reinterpret_cast<const __nv_bfloat16 *>(&v);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) S[rv + i][kk] = h[i];
+    }
+  } else if (sk <= sr) {       // k varies fastest across threads
+    for (int e = tid; e < 128 * GK; e += 256) {
+      const int rr = e / GK, kk = e % GK;
+      const int r = r0 + rr, k = k0 + kk;
+      S[rr][kk] = (r < nrows && k < K) ? X[(long long)r * sr + (long long)k * sk] : zero;
+    }
+  } else {                     // rows vary fastest across threads
+    for (int e = tid; e < 128 * GK; e += 256) {
+      const int kk = e / 128, rr = e % 128;
+      const int r = r0 + rr, k = k0 + kk;
+      S[rr][kk] = (r < nrows && k < K) ? X[(long long)r * sr + (long long)k * sk] : zero;
+    }
+  }
+}
+
+// 256 threads = 8 warps; warp w computes rows (w % 4) * 32 .. +32 and columns (w / 4) * 64
+// .. +64 of the block's 128 x 128 tile: 2 x 8 tensor-core tiles per 16-wide k step.
 __global__ void __launch_bounds__(256) k_gemm_bf16(const __nv_bfloat16 *__restrict__ A, long long sam, long long sak,
                                                    const __nv_bfloat16 *__restrict__ B, long long sbn, long long sbk,
                                                    float *__restrict__ C, long long ldc, int M, int N, int K,
                                                    const float *__restrict__ bias, __nv_bfloat16 *__restrict__ Y,
                                                    long long ldy, int act, int accumulate) {
-  __shared__ float As[TK][TM + 1];
-  __shared__ float Bs[TK][TN + 1];
-  const int tid = threadIdx.x;
-  const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
-  const int tr = tid / 16, tc = tid % 16;   // 16 x 16 threads, 4x4 outputs each
-  float acc[4][4];
+  __shared__ __align__(16) __nv_bfloat16 As[GM][GKP];
+  __shared__ __align__(16) __nv_bfloat16 Bs[GN][GKP];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = (warp & 3) * 32, wn = (warp >> 2) * 64;
+  const int m0 = blockIdx.y * GM, n0 = blockIdx.x * GN;
+  const int g = lane >> 2, t = lane & 3;
+  const bool a16 = (reinterpret_cast<uintptr_t>(A) & 15) == 0, b16 = (reinterpret_cast<uintptr_t>(B) & 15) == 0;
+  const bool avk = a16 && sak == 1 && sam % 8 == 0 && K % 8 == 0;
+  const bool avr = a16 && !avk && sam == 1 && sak % 8 == 0 && M % 8 == 0;
+  const bool bvk = b16 && sbk == 1 && sbn % 8 == 0 && K % 8 == 0;
+  const bool bvr = b16 && !bvk && sbn == 1 && sbk % 8 == 0 && N % 8 == 0;
+  float acc[2][8][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
-  for (int k0 = 0; k0 < K; k0 += TK) {
-    for (int e = tid; e < TK * TM; e += 256) {
-      const int kk = e / TM, mm = e % TM;
-      const int m = m0 + mm, k = k0 + kk;
-      As[kk][mm] = (m < M && k < K) ? __bfloat162float(A[m * sam + k * sak]) : 0.f;
-    }
-    for (int e = tid; e < TK * TN; e += 256) {
-      const int kk = e / TN, nn = e % TN;
-      const int n = n0 + nn, k = k0 + kk;
-      Bs[kk][nn] = (n < N && k < K) ? __bfloat162float(B[n * sbn + k * sbk]) : 0.f;
-    }
+    for (int j = 0; j < 8; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
+  for (int k0 = 0; k0 < K; k0 += GK) {
+    stage_tile(A, sam, sak, m0, M, k0, K, avk, avr, As);
+    stage_tile(B, sbn, sbk, n0, N, k0, K, bvk, bvr, Bs);
     __syncthreads();
 #pragma unroll
-    for (int kk = 0; kk < TK; ++kk) {
-      float a[4], b[4];
+    for (int ks = 0; ks < GK; ks += 16) {
+      uint32_t af[2][4], bf[8][2];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][tr * 4 + i];
+      for (int i = 0; i < 2; ++i) {
+        const int r = wm + i * 16 + g;
+        af[i][0] = *reinterpret_cast<const uint32_t *>(&As[r][ks + 2 * t]);
+        af[i][1] = *reinterpret_cast<const uint32_t *>(&As[r + 8][ks + 2 * t]);
+        af[i][2] = *reinterpret_cast<const uint32_t *>(&As[r][ks + 2 * t + 8]);
+        af[i][3] = *reinterpret_cast<const uint32_t *>(&As[r + 8][ks + 2 * t + 8]);
+      }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tc * 4 + j];
+      for (int j = 0; j < 8; ++j) {
+        const int c = wn + j * 8 + g;
+        bf[j][0] = *reinterpret_cast<const uint32_t *>(&Bs[c][ks + 2 * t]);
+        bf[j][1] = *reinterpret_cast<const uint32_t *>(&Bs[c][ks + 2 * t + 8]);
+      }
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+        for (int j = 0; j < 8; ++j) mma_16816(acc[i][j], af[i], bf[j]);
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int m = m0 + tr * 4 + i, n = n0 + tc * 4 + j;
-      if (m >= M || n >= N) continue;
-      float z = acc[i][j] + (bias ? bias[n] : 0.f);
-      if (accumulate) z += C[m * ldc + n];
-      C[m * ldc + n] = z;
-      if (Y) Y[m * ldy + n] = __float2bfloat16(act ? silu(z) : z);
-    }
+    for (int j = 0; j < 8; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int m = m0 + wm + i * 16 + g + (q >> 1) * 8, n = n0 + wn + j * 8 + 2 * t + (q & 1);
+        if (m >= M || n >= N) continue;
+        float z = acc[i][j][q] + (bias ? bias[n] : 0.f);
+        if (accumulate) z += C[m * ldc + n];
+        C[m * ldc + n] = z;
+        if (Y) Y[m * ldy + n] = __float2bfloat16(act ? silu(z) : z);
+      }
 }
 
 __global__ void k_silu_bwd(const float *__restrict__ dY, const float *__restrict__ Z, __nv_bfloat16 *__restrict__ dZ,
@@ -147,7 +215,8 @@ cqg_status cqg_mlp_gemm_bf16(const void *A, long long sam, long long sak, const 
                              int act, int accumulate, void *stream) {
   if (!A || !B || !C || M < 0 || N < 0 || K < 0) return CQG_ERR_BAD_ARG;
   if (M == 0 || N == 0) return CQG_OK;
-  dim3 grid((N + TN - 1) / TN, (M + TM - 1) / TM);
+  if ((M + GM - 1) / GM > 65535) return CQG_ERR_BAD_ARG;   // grid.y limit: M <= 8.4 M rows
+  dim3 grid((N + GN - 1) / GN, (M + GM - 1) / GM);
   k_gemm_bf16<<<grid, 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)A, sam, sak, (const __nv_bfloat16 *)B,
                                                       sbn, sbk, C, ldc, M, N, K, bias, (__nv_bfloat16 *)Y, ldy, act,
                                                       accumulate);

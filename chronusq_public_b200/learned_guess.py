@@ -16,6 +16,7 @@ Run as ``python -m chronusq_public_b200.learned_guess --basis 6-31g* --train 400
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import time
 from typing import Dict, List, Sequence
@@ -88,6 +89,65 @@ def train(basis: str = "6-31g*", ntrain: int = 4000, nmin: int = 2, nmax: int = 
             "loss_last": hist[-1], "mean_scf_iterations_sad": float(its.mean()), "model": model}
 
 
+def training_throughput(pairs: int = 692570, epochs: int = 2, width: int = 256, layers: int = 4,
+                        batch: int = 2048, seed: int = 0) -> Dict:
+    """Speed of the network's training on the GPU with the library's kernels, on random
+    inputs of the shipped training set's shape (`pairs` rows): seconds per epoch and the
+    GEMM FLOPs per epoch over that time (forward, weight gradients, input gradients of
+    every layer but the first), plus one large forward GEMM (all rows, width x width) timed
+    alone, each against the measured dense BF16 peak when known."""
+    import torch
+    from .guess_model import NFEAT, MAXF
+    from . import _lib
+    rng = np.random.default_rng(seed)
+    X = rng.normal(size=(pairs, NFEAT)).astype(np.float32)
+    X[:, -1] = 1.0
+    T = rng.normal(size=(pairs, MAXF * MAXF)).astype(np.float32)
+    M = np.ones_like(T)
+    model = PairMLP(width=width, layers=layers, seed=seed)
+    model.fit(X[:batch * 4], T[:batch * 4], M[:batch * 4], epochs=1, batch=batch)     # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    model.fit(X, T, M, epochs=epochs, batch=batch)
+    torch.cuda.synchronize()
+    sec = (time.perf_counter() - t0) / epochs
+    kn = [a * b for a, b in zip(model.dims[:-1], model.dims[1:])]
+    flops = 2.0 * pairs * (2 * sum(kn) + sum(kn[1:]))
+    # one forward GEMM over all rows, width -> width, alone
+    A = torch.randn((pairs, width), device="cuda").to(torch.bfloat16)
+    B = torch.randn((width, width), device="cuda").to(torch.bfloat16)
+    C = torch.empty((pairs, width), device="cuda")
+    L = _lib.lib()
+    args = [ctypes.c_void_p(A.data_ptr()), width, 1, ctypes.c_void_p(B.data_ptr()), width, 1,
+            ctypes.c_void_p(C.data_ptr()), width, pairs, width, width, None, None, 0, 0, 0, None]
+    for _ in range(3):
+        _lib.check(L.cqg_mlp_gemm_bf16(*args))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        _lib.check(L.cqg_mlp_gemm_bf16(*args))
+    e1.record()
+    torch.cuda.synchronize()
+    gemm_s = e0.elapsed_time(e1) / 10 * 1e-3
+    gemm_tf = 2.0 * pairs * width * width / gemm_s / 1e12
+    peak = None
+    try:
+        import json as _json
+        import os as _os
+        pp = _os.path.join(_os.path.dirname(_os.path.dirname(_os.path.abspath(__file__))), "MEASURED_PEAKS.json")
+        peak = float(_json.load(open(pp))["bf16_tflops"])
+    except (OSError, ValueError, KeyError):
+        peak = None
+    out = {"pairs": pairs, "batch": batch, "dims": model.dims, "seconds_per_epoch": sec,
+           "gemm_tflop_per_epoch": flops / 1e12, "training_tflops": flops / sec / 1e12,
+           "gemm_alone": {"shape": [pairs, width, width], "ms": gemm_s * 1e3, "tflops": gemm_tf},
+           "bf16_peak_tflops": peak}
+    if peak:
+        out["training_frac_of_peak"] = out["training_tflops"] / peak
+        out["gemm_alone"]["frac_of_peak"] = gemm_tf / peak
+    return out
+
+
 def evaluate(model: PairMLP, basis: str = "6-31g*", nheld: int = 500, nmin: int = 2, nmax: int = 16,
              seed: int = 8, single: int = 32, thresh: float = 1e-12) -> Dict:
     """Held-out clusters (a seed disjoint from training) converged to the reference's
@@ -106,8 +166,11 @@ def evaluate(model: PairMLP, basis: str = "6-31g*", nheld: int = 500, nmin: int 
         res["batched_%s_mean_iterations" % name] = float(b.iterations.mean())
         res["batched_%s_max_iterations" % name] = int(b.iterations.max())
         res["batched_%s_converged" % name] = bool(b.converged)
+        res["batched_%s_guess_seconds" % name] = b.guess_seconds
+        res["batched_%s_fock_seconds" % name] = b.fock_seconds
         if mdl is not None:
             res["batched_learned_fallbacks"] = int(b.guess_fallbacks)
+            res["batched_learned_predict_seconds"] = b.predict_seconds
         else:
             # guess quality: distance of the starting densities from the converged ones
             P0, _ = b.learned_density(model)
