@@ -184,10 +184,12 @@ def _aname(members, mb, mk, i):
     return "acc%d_%d_%d" % (mb, mk, i) if members else "acc%d" % i
 
 
-def _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members=None):
+def _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members=None, nkt=1):
     """One pass over `nbt` bra primitive pairs starting at bra[ib]: their E coefficients,
     the ket loop (each ket primitive pair loaded and its E coefficients built once for
-    all nbt bra primitives), and the bra transforms into acc.
+    all nbt bra primitives; with nkt > 1, nkt ket primitive pairs per iteration, whose
+    Boys / R chains are independent, then a one-at-a-time remainder), and the bra
+    transforms into acc.
 
     members = (mb, mk) emits the sibling form: the primitive pairs carry unit contraction
     coefficients, bw[m * nbra + i] / kw[m * nket + i] are member m's coefficient products,
@@ -213,51 +215,52 @@ def _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members=No
             for h in range(len(hp)):
                 for c in range(ncd):
                     g.w("T %s = T(0);" % _wname(members, j, m, h, c))
-    g.w("PrimPair pk_next;")
-    g.w("if (nket > 0) pk_next = ket[0];")
-    g.w("for (int ik = 0; ik < nket; ++ik) {")
-    g.ind += 1
-    g.w("const PrimPair pk = pk_next;")
-    g.w("if (ik + 1 < nket) pk_next = ket[ik + 1];")
-    g.w("const double q = pk.p;")
-    g.w("const T ko2p = T(0.5 * pk.ip);")
-    if members:
-        for m in range(mk):
-            g.w("const T kw%d = T(kw[%d * nket + ik]);" % (m, m))
-    for d in "xyz":
-        g.w("const T kPA%s = T(pk.P%s - C.%s);" % (d, d, d))
-        g.w("const T kPB%s = T(pk.P%s - D.%s);" % (d, d, d))
     needk = {d: set() for d in "xyz"}
     for c in cc:
         for dd in cd:
             for k, d in enumerate("xyz"):
                 needk[d].add((c[k], dd[k]))
-    emit_E(g, "k", lc, ld, needk)
-    # ket Hermite coefficients shared by the nbt bra primitives
-    kterms = []
-    ci = 0
-    for c in cc:
-        for dd in cd:
-            for (tnp, fac) in herm_terms("k", c, dd):
-                sgn = -1 if (sum(tnp) % 2) else 1
-                coef = " * ".join(fac) if fac else None
-                cname = "kc_%d_%d_%d_%d" % (ci, tnp[0], tnp[1], tnp[2])
-                cexpr = ("T(%d)" % sgn) if coef is None else (("-" if sgn < 0 else "") + "(" + coef + ")")
-                g.w("const T %s = %s;" % (cname, cexpr))
-                kterms.append((ci, tnp, cname))
-            ci += 1
-    for j in range(nbt):
-        r = "r%d_" % j
+
+    def ket_quantities(ktag, qname, kcp):
+        """Ket primitive pair p<ktag>: its exponent, E coefficients and the signed ket
+        Hermite coefficients kc (shared by the nbt bra primitives)."""
+        g.w("const double %s = p%s.p;" % (qname, ktag))
+        g.w("const T %so2p = T(0.5 * p%s.ip);" % (ktag, ktag))
+        if members:
+            for m in range(mk):
+                g.w("const T kw%d = T(kw[%d * nket + ik]);" % (m, m))
+        for d in "xyz":
+            g.w("const T %sPA%s = T(p%s.P%s - C.%s);" % (ktag, d, ktag, d, d))
+            g.w("const T %sPB%s = T(p%s.P%s - D.%s);" % (ktag, d, ktag, d, d))
+        emit_E(g, ktag, lc, ld, needk)
+        kterms = []
+        ci = 0
+        for c in cc:
+            for dd in cd:
+                for (tnp, fac) in herm_terms(ktag, c, dd):
+                    sgn = -1 if (sum(tnp) % 2) else 1
+                    coef = " * ".join(fac) if fac else None
+                    cname = "%s%d_%d_%d_%d" % (kcp, ci, tnp[0], tnp[1], tnp[2])
+                    cexpr = ("T(%d)" % sgn) if coef is None else (("-" if sgn < 0 else "") + "(" + coef + ")")
+                    g.w("const T %s = %s;" % (cname, cexpr))
+                    kterms.append((ci, tnp, cname))
+                ci += 1
+        return kterms
+
+    def chain(j, ktag, qname, kterms, r):
+        """One primitive quartet (bra primitive j, ket primitive p<ktag>): Boys values, the R
+        recursion and the ket transform into W."""
         g.w("{")
         g.ind += 1
-        g.w("const double pq = p%d + q;" % j)
+        g.w("const double pq = p%d + %s;" % (j, qname))
         g.w("const double rpq = rsqrt(pq);")
-        g.w("const double rho = p%d * q * (rpq * rpq);" % j)
-        g.w("const double PQx = pb%d.Px - pk.Px, PQy = pb%d.Py - pk.Py, PQz = pb%d.Pz - pk.Pz;" % (j, j, j))
+        g.w("const double rho = p%d * %s * (rpq * rpq);" % (j, qname))
+        g.w("const double PQx = pb%d.Px - p%s.Px, PQy = pb%d.Py - p%s.Py, PQz = pb%d.Pz - p%s.Pz;"
+            % (j, ktag, j, ktag, j, ktag))
         g.w("const double Tb = rho * (PQx * PQx + PQy * PQy + PQz * PQz);")
         g.w("double F[%d];" % (L + 1))
         g.w("boys_eval_sm<%d>(Tb, boys_tab, F);" % L)
-        g.w("double fac = pb%d.Kp * pk.Kp * rpq;" % j)
+        g.w("double fac = pb%d.Kp * p%s.Kp * rpq;" % (j, ktag))
         if L > 0:
             g.w("const double m2r = -2.0 * rho;")
         for n in range(L + 1):
@@ -300,6 +303,35 @@ def _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members=No
                     g.w("}")
         g.ind -= 1
         g.w("}")
+
+    if nkt > 1 and not members:
+        # ket primitive pairs nkt at a time: nkt independent Boys / R chains per bra primitive
+        g.w("int ik = 0;")
+        g.w("for (; ik + %d < nket; ik += %d) {" % (nkt - 1, nkt))
+        g.ind += 1
+        tiles = []
+        for m in range(nkt):
+            g.w("const PrimPair pk%d = ket[ik + %d];" % (m, m))
+        for m in range(nkt):
+            tiles.append(ket_quantities("k%d" % m, "qk%d" % m, "kc%d_" % m))
+        for j in range(nbt):
+            for m in range(nkt):
+                chain(j, "k%d" % m, "qk%d" % m, tiles[m], "r%dk%d_" % (j, m))
+        g.ind -= 1
+        g.w("}")
+        g.w("PrimPair pk_next;")
+        g.w("if (ik < nket) pk_next = ket[ik];")
+        g.w("for (; ik < nket; ++ik) {")
+    else:
+        g.w("PrimPair pk_next;")
+        g.w("if (nket > 0) pk_next = ket[0];")
+        g.w("for (int ik = 0; ik < nket; ++ik) {")
+    g.ind += 1
+    g.w("const PrimPair pk = pk_next;")
+    g.w("if (ik + 1 < nket) pk_next = ket[ik + 1];")
+    kterms = ket_quantities("k", "q", "kc_")
+    for j in range(nbt):
+        chain(j, "k", "q", kterms, "r%d_" % j)
     g.ind -= 1
     g.w("}")
     # bra transform: acc[ab][cd] += sum_tuv Eab_tuv W[tuv][cd]
@@ -329,7 +361,7 @@ def _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members=No
                 ai += 1
 
 
-def gen_class(la, lb, lc, ld, pa, pb, pc, pd, nbt=1, members=None):
+def gen_class(la, lb, lc, ld, pa, pb, pc, pd, nbt=1, members=None, nkt=1):
     """Device function of one class; nbt > 1 walks the bra primitive pairs nbt at a time
     (each ket primitive pair is then read once per nbt bra primitives), with a one-at-a-time
     loop for the remainder.
@@ -366,12 +398,12 @@ def gen_class(la, lb, lc, ld, pa, pb, pc, pd, nbt=1, members=None):
     if nbt > 1:
         g.w("for (; ib + %d < nbra; ib += %d) {" % (nbt - 1, nbt))
         g.ind += 1
-        _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members)
+        _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members, nkt)
         g.ind -= 1
         g.w("}")
     g.w("for (; ib < nbra; ++ib) {")
     g.ind += 1
-    _emit_tile(g, 1, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members)
+    _emit_tile(g, 1, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members, nkt)
     g.ind -= 1
     g.w("}")
     # spherical transform, axis by axis: cart arrays named by index tuples
@@ -449,6 +481,13 @@ WARP_CLASSES = {q for q in quartet_classes(3)
 # slower with 2 (register pressure), so they keep one.
 BRA_TILE = {(0, 0, 0, 0): 4}
 
+# classes whose ket primitive pairs are walked several at a time within each bra primitive
+# (independent chains of Boys values and R recursion per iteration).  Measured on (H2O)_32
+# cc-pVDZ and rejected: two ket primitives per iteration made (ps|ss), (ps|ps), (pp|ss),
+# (ds|ss), (pp|ps), (ds|ps) 5-11 % slower, and (ss|ss) with 2 bra x 2 ket instead of 4 bra
+# 18 % slower; so no class uses it.
+KET_TILE = {}
+
 
 def members_header(specs):
     """Header text with the sibling-member variants for `specs` = [(la, lb, lc, ld, mb, mk)],
@@ -487,7 +526,7 @@ def main(path, maxl=2):
         if (la, lb, lc, ld) in WARP_CLASSES:
             continue
         _, code = gen_class(la, lb, lc, ld, la > 1, lb > 1, lc > 1, ld > 1,
-                            nbt=BRA_TILE.get((la, lb, lc, ld), 1))
+                            nbt=BRA_TILE.get((la, lb, lc, ld), 1), nkt=KET_TILE.get((la, lb, lc, ld), 1))
         parts.append(code)
         parts.append("template <> struct EriClass<%d, %d, %d, %d> {" % (la, lb, lc, ld))
         parts.append("  template <typename T> static __device__ __forceinline__ void run(const PrimPair* bra, int nbra,"
