@@ -261,17 +261,26 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+FUSED_TIER1 = {"(ss|ss)", "(ps|ss)"}
+WARP_TO_DD = {"(dp|pp)", "(dp|dp)", "(dd|pp)", "(dd|ds)", "(dd|dp)", "(dd|dd)"}   # warp-only classes to (dd|dd)
+
+
 def schedule_summary(ints, st):
-    """The autotuned schedule of the lists that had work: per class, the kernel form, CTAs
-    per SM, warps per CTA and quartets claimed per warp."""
+    """The autotuned schedule of the lists that had work: per class, the kernel form (one
+    quartet per thread, warp-cooperative, or inside the class-fused kernel), CTAs per SM,
+    warps per CTA, quartets claimed per warp and the class kernel's time; plus the fusion
+    tier in use, the fused kernel's time and the autotuner's times of the three tiers."""
     sch = ints.schedule()
-    out = {}
+    tier, tuned = ints.fusion()
+    out = {"fusion": {"tier": tier, "fused_kernel_ms": round(st.get("ms_fused", 0.0), 4),
+                      "tuned_ms_tier0_1_2": [round(x, 4) for x in tuned]}}
     for k, (name, nq) in enumerate(st["class_quartets"].items()):
         if nq <= 0:
             continue
-        out[name] = {"form": "warp" if sch["warp_form"][k] else "thread", "cta_per_sm": sch["cta_per_sm"][k],
-                     "warps_per_cta": sch["warps_per_cta"][k], "quartets_per_warp": sch["quartets_per_warp"][k],
-                     "ms": round(st["class_ms"][name], 4)}
+        fused = (tier == 1 and name in FUSED_TIER1) or (tier == 2 and name not in WARP_TO_DD and "f" not in name)
+        form = "fused" if fused else ("warp" if sch["warp_form"][k] else "thread")
+        out[name] = {"form": form, "cta_per_sm": sch["cta_per_sm"][k], "warps_per_cta": sch["warps_per_cta"][k],
+                     "quartets_per_warp": sch["quartets_per_warp"][k], "ms": round(st["class_ms"][name], 4)}
     return out
 
 
@@ -428,6 +437,8 @@ def main():
     ap.add_argument("--no-sweep", action="store_true", help="skip the FP32 cutoff sweep 1e-10..1e-6")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes instead of autotuned ones")
+    ap.add_argument("--fusion", default="auto", choices=["auto", "0", "1", "2"],
+                    help="class-fusion tier of the benchmarked builds (auto: the autotuner's choice)")
     ap.add_argument("--schedule-out", default=None, help="write the autotuned per-list schedule to this JSON file")
     ap.add_argument("--schedule-in", default=None,
                     help="use the per-list schedule in this JSON file (from --schedule-out) instead of autotuning")
@@ -468,15 +479,19 @@ def main():
     stream = torch.cuda.current_stream()
 
     if args.schedule_in:
-        ints.setSchedule(**json.load(open(args.schedule_in)))
+        sch = json.load(open(args.schedule_in))
+        ints.setSchedule(**{k: sch[k] for k in ("cta_per_sm", "warps_per_cta", "quartets_per_warp", "warp_form")})
+        ints.setFusion(int(sch.get("fusion_tier", 0)))
     elif not args.no_autotune:
         ints.autotune_next()              # the first warm-up build picks every class's launch shape
-    for _ in range(args.warmup):
+    for i in range(args.warmup):
         ints.formPT(Dd, PTs=PT)
+        if i == 0 and args.fusion != "auto":
+            ints.setFusion(int(args.fusion))
     torch.cuda.synchronize()
     if args.schedule_out and rank == 0:
         with open(args.schedule_out, "w") as f:
-            json.dump(ints.schedule(), f)
+            json.dump(dict(ints.schedule(), fusion_tier=ints.fusion()[0]), f)
     ints.setTiming(True)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     step_ms, eri_ms, quartets, mflops, launches, class_ms = [], [], [], [], 0, {}

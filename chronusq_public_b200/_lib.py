@@ -34,6 +34,7 @@ EXPORTED = [
     "cqg_set_graph_mode", "cqg_graph_status", "cqg_autotune_next", "cqg_get_launch_shapes", "cqg_set_active",
     "cqg_mlp_gemm_bf16", "cqg_mlp_silu_bwd", "cqg_mlp_to_bf16", "cqg_mlp_colsum", "cqg_mlp_mse", "cqg_mlp_adam",
     "cqg_one_e_noalloc", "cqg_dipole", "cqg_get_schedule", "cqg_set_schedule",
+    "cqg_set_fusion", "cqg_get_fusion", "cqg_mlp_adam_dev",
 ]
 
 
@@ -51,6 +52,8 @@ class CqgStats(ctypes.Structure):
         ("chunks", ctypes.c_longlong),
         ("class_quartets", ctypes.c_longlong * 55),
         ("class_ms", ctypes.c_double * 55),
+        ("ms_fused", ctypes.c_double),
+        ("fused_tier", ctypes.c_int),
     ]
 
 
@@ -92,6 +95,8 @@ def load(path: str = LIB_PATH):
     L.cqg_get_launch_shapes.argtypes = [vp, i, i]
     L.cqg_get_schedule.argtypes = [vp, i, i, i, i]
     L.cqg_set_schedule.argtypes = [vp, i, i, i, i]
+    L.cqg_set_fusion.argtypes = [vp, ctypes.c_int]
+    L.cqg_get_fusion.argtypes = [vp, i, d]
     L.cqg_set_active.argtypes = [vp, ctypes.c_char_p]
     ll, f, fp = ctypes.c_longlong, ctypes.c_float, ctypes.POINTER(ctypes.c_float)
     L.cqg_mlp_gemm_bf16.argtypes = [vp, ll, ll, vp, ll, ll, vp, ll, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp,
@@ -101,6 +106,7 @@ def load(path: str = LIB_PATH):
     L.cqg_mlp_colsum.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp]
     L.cqg_mlp_mse.argtypes = [vp, vp, vp, ll, f, vp, vp, vp]
     L.cqg_mlp_adam.argtypes = [vp, vp, vp, vp, ll, f, f, f, f, ctypes.c_int, f, vp, vp]
+    L.cqg_mlp_adam_dev.argtypes = [vp, vp, vp, vp, ll, vp, f, f, f, f, vp, vp]
     L.cqg_class_name.argtypes = [ctypes.c_int]
     L.cqg_class_name.restype = ctypes.c_char_p
     L.cqg_probe_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, d]
@@ -114,7 +120,7 @@ def load(path: str = LIB_PATH):
                  "cqg_twoe_contract_direct_batch", "cqg_one_e_batch", "cqg_set_graph_mode",
                  "cqg_graph_status", "cqg_autotune_next", "cqg_get_launch_shapes", "cqg_set_active",
                  "cqg_mlp_gemm_bf16", "cqg_mlp_silu_bwd", "cqg_mlp_to_bf16", "cqg_mlp_colsum", "cqg_mlp_mse",
-                 "cqg_mlp_adam", "cqg_one_e_noalloc", "cqg_dipole", "cqg_get_schedule", "cqg_set_schedule"]:
+                 "cqg_mlp_adam", "cqg_one_e_noalloc", "cqg_dipole", "cqg_get_schedule", "cqg_set_schedule", "cqg_set_fusion", "cqg_get_fusion", "cqg_mlp_adam_dev"]:
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

@@ -136,6 +136,18 @@ class AOIntegrals:
         _lib.check(self._L.cqg_get_schedule(self._ctx, *out), self._ctx)
         return {k: list(v) for k, v in zip(("cta_per_sm", "warps_per_cta", "quartets_per_warp", "warp_form"), out)}
 
+    def setFusion(self, tier: int):
+        """0: one launch per class list; 1 / 2: the light / all per-thread classes up to
+        (dd|dd) in one class-fused persistent kernel fed by a device work queue."""
+        _lib.check(self._L.cqg_set_fusion(self._ctx, int(tier)), self._ctx)
+
+    def fusion(self):
+        """(tier in use, the autotuner's times in ms of tiers 0, 1, 2; zeros before tuning)."""
+        t = ctypes.c_int()
+        ms = (ctypes.c_double * 3)()
+        _lib.check(self._L.cqg_get_fusion(self._ctx, ctypes.byref(t), ms), self._ctx)
+        return int(t.value), list(ms)
+
     def setSchedule(self, cta_per_sm=None, warps_per_cta=None, quartets_per_warp=None, warp_form=None):
         """Set the per-list schedule (sequences of 110 ints as :meth:`schedule` returns them,
         or one int for every list; None leaves that part unchanged)."""
@@ -169,6 +181,7 @@ class AOIntegrals:
             "launches": int(s.launches), "chunks": int(s.chunks),
             "class_quartets": {names[k]: int(s.class_quartets[k]) for k in range(len(names))},
             "class_ms": {names[k]: float(s.class_ms[k]) for k in range(len(names))},
+            "ms_fused": float(s.ms_fused), "fused_tier": int(s.fused_tier),
         }
 
     # ------------------------------------------------------------------ contraction ---

@@ -4,8 +4,8 @@
 
 Steps: generate the per-class ERI code (csrc/gen_eri.py -> csrc/_gen/eri_classes.cuh),
 compile the translation units in parallel -- csrc/engine.cu (C ABI, screening, list build),
-csrc/mlp.cu (learned-guess kernels) and csrc/eri_part.cu once per share of the quartet
-classes (-DCQG_PART=0..NPART-1) -- and link them with nvcc into
+csrc/mlp.cu (learned-guess kernels), csrc/eri_part.cu once per share of the quartet
+classes (-DCQG_PART=0..NPART-1) and csrc/eri_fused.cu (the class-fused kernel) -- and link them with nvcc into
 chronusq_public_b200/libcqgpu.so.  The build is skipped when the library is newer than
 every source.
 """
@@ -58,6 +58,7 @@ def build(force: bool = False, verbose: bool = True, extra_flags=()) -> str:
     os.makedirs(objdir, exist_ok=True)
     units = [("engine", os.path.join(CSRC, "engine.cu"), []), ("mlp", os.path.join(CSRC, "mlp.cu"), [])]
     units += [("eri_part%d" % k, os.path.join(CSRC, "eri_part.cu"), ["-DCQG_PART=%d" % k]) for k in range(NPART)]
+    units += [("eri_fused", os.path.join(CSRC, "eri_fused.cu"), [])]
     jobs = []
     for name, src, defs in units:
         obj = os.path.join(objdir, name + ".o")

@@ -207,7 +207,7 @@ cqg_status cqg_create(cqg_ctx **out, int device) {
     delete ctx;
     return CQG_ERR_CUDA;
   }
-  for (int i = 0; i < 4 + 2 * 55; ++i) cudaEventCreate(&ctx->ev[i]);
+  for (int i = 0; i < 4 + 2 * 55 + 2; ++i) cudaEventCreate(&ctx->ev[i]);
   ctx->events = true;
   cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
   *out = ctx;
@@ -230,7 +230,7 @@ cqg_status cqg_destroy(cqg_ctx *ctx) {
   ctx->d_qhead.release();
   ctx->d_qlist.release(); ctx->d_G.release(); ctx->d_X.release(); ctx->d_AX.release(); ctx->d_Gscratch.release();
   if (ctx->events)
-    for (int i = 0; i < 4 + 2 * 55; ++i) cudaEventDestroy(ctx->ev[i]);
+    for (int i = 0; i < 4 + 2 * 55 + 2; ++i) cudaEventDestroy(ctx->ev[i]);
   delete ctx;
   return CQG_OK;
 }
@@ -511,7 +511,7 @@ cqg_status cqg_set_basis_batch(cqg_ctx *ctx, int nmol, const int *nshell_per_mol
   size_t scan_bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (long long *)nullptr, (long long *)nullptr, std::max(2 * task, 1));
   if (ctx->d_cnt.reserve(2 * task + 1) || ctx->d_off.reserve(2 * task + 1) || ctx->d_range.reserve(4 * CQG_NQC) ||
-      ctx->d_qhead.reserve(2 * CQG_NQC) ||
+      ctx->d_qhead.reserve(2 * CQG_NQC + 1) ||
       ctx->d_scan_tmp.reserve(scan_bytes + 16) || ctx->d_M.reserve(2 * (size_t)std::max(ctx->Mtotal, 1LL)) ||
       ctx->d_Mmax.reserve(1) || ctx->d_flags.reserve(4) || ctx->d_blkacc.reserve(4 * CQG_NQC))
     return CQG_ERR_OOM;
@@ -528,6 +528,14 @@ cqg_status cqg_get_schwarz(cqg_ctx *ctx, double *Q) {
   if (ctx->nshell == 0) return CQG_ERR_STATE;
   memcpy(Q, ctx->Qmat.data(), ctx->Qmat.size() * sizeof(double));
   return CQG_OK;
+}
+
+// Whether quartet class k goes through the class-fused kernel of `tier` (0: none).
+static bool class_fused(int tier, int k) {
+  if (tier == 0) return false;
+  int i, j;
+  qclass_split(k, i, j);
+  return cqg_fused_member(tier, kPairClass[i][0], kPairClass[i][1], kPairClass[j][0], kPairClass[j][1]);
 }
 
 // Launch-shape autotuner: for every (precision, class) list with work, time each candidate
@@ -612,6 +620,48 @@ static cqg_status autotune_shapes(cqg_ctx *ctx, const long long *crange, cudaStr
     ctx->shape_qpw[vb] = pick.qpw;
     ctx->shape_var[vb] = pick.var;
   }
+  // Class fusion: the lists of the tier-2 classes (every per-thread class up to (dd|dd)) as
+  // one launch per list with the shapes just tuned, as the tier-1 fused kernel plus per-list
+  // launches of the rest, and as the tier-2 fused kernel; full lists, each timed after one
+  // untimed run; the fastest is kept.
+  bool any = false;
+  for (int vb = 0; vb < 2 * CQG_NQC; ++vb)
+    if (crange[2 * vb + 1] > crange[2 * vb] && class_fused(2, vb % CQG_NQC)) any = true;
+  if (any) {
+    float best = 1e30f;
+    int pick = 0;
+    for (int tier = 0; tier <= 2; ++tier) {
+      float t = 1e30f;
+      for (int rep = 0; rep < 2; ++rep) {
+        CUCHK(cudaMemsetAsync(ctx->d_qhead.p, 0, 2 * CQG_NQC * sizeof(unsigned long long), st));
+        cudaEventRecord(e0, st);
+        cudaError_t e = tier ? cqg_launch_fused(ctx, tier, st, scratch) : cudaSuccess;
+        for (int vb = 0; vb < 2 * CQG_NQC && e == cudaSuccess; ++vb) {
+          const int k = vb % CQG_NQC;
+          const long long n = crange[2 * vb + 1] - crange[2 * vb];
+          if (n <= 0 || !class_fused(2, k) || class_fused(tier, k)) continue;
+          e = (vb < CQG_NQC ? kEriLaunch[k] : kEriLaunch32[k])(ctx, vb, n, st, scratch);
+        }
+        cudaEventRecord(e1, st);
+        if (e != cudaSuccess) {
+          cudaEventDestroy(e0);
+          cudaEventDestroy(e1);
+          ctx->err = std::string("autotune (class fusion): ") + cudaGetErrorString(e);
+          return CQG_ERR_CUDA;
+        }
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep == 1) t = ms;
+      }
+      ctx->fusion_ms[tier] = t;
+      if (t < best) {
+        best = t;
+        pick = tier;
+      }
+    }
+    ctx->fused_tier = pick;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return CQG_OK;
@@ -672,8 +722,16 @@ static cqg_status contract_graph(cqg_ctx *ctx, int ngroups, const double *const 
   }
   CUCHK(cudaMemsetAsync(ctx->d_qhead.p, 0, 2 * CQG_NQC * sizeof(unsigned long long), st));
   int launches = 6;
+  if (ctx->fused_tier) {
+    cudaError_t e = cqg_launch_fused(ctx, ctx->fused_tier, st, dg);
+    ++launches;
+    if (e != cudaSuccess) {
+      ctx->err = std::string("class-fused eri kernel: ") + cudaGetErrorString(e);
+      return CQG_ERR_CUDA;
+    }
+  }
   for (int k = 0; k < CQG_NQC; ++k) {
-    if (!ctx->class_possible[k]) continue;
+    if (!ctx->class_possible[k] || class_fused(ctx->fused_tier, k)) continue;
     cudaError_t e = kEriLaunch[k](ctx, k, -1, st, dg);
     ++launches;
     if (e == cudaSuccess && ctx->policy == CQG_PREC_MIXED) {
@@ -809,6 +867,8 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
   }
   memset(ctx->stats.class_quartets, 0, sizeof(ctx->stats.class_quartets));
   memset(ctx->stats.class_ms, 0, sizeof(ctx->stats.class_ms));
+  ctx->stats.ms_fused = 0.0;
+  ctx->stats.fused_tier = ctx->fused_tier;
   double mflops = 0, mflops32 = 0;
   long long nprimq = 0, nq32 = 0;
   for (int k = 0; k < CQG_NQC; ++k) {
@@ -866,7 +926,18 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     }
     // 3. ERI + digest per class, each list consumed through its work-queue head counter
     CUCHK(cudaMemsetAsync(ctx->d_qhead.p, 0, 2 * CQG_NQC * sizeof(unsigned long long), st));
+    if (ctx->fused_tier) {   // the fused tier's lists in one launch (its time: ms_fused)
+      if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[4 + 2 * CQG_NQC], st));
+      cudaError_t e = cqg_launch_fused(ctx, ctx->fused_tier, st, dg);
+      if (e != cudaSuccess) {
+        ctx->err = std::string("class-fused eri kernel: ") + cudaGetErrorString(e);
+        return CQG_ERR_CUDA;
+      }
+      if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[5 + 2 * CQG_NQC], st));
+      ctx->launches += 1;
+    }
     for (int k = 0; k < CQG_NQC; ++k) {
+      if (class_fused(ctx->fused_tier, k)) continue;
       const long long n64 = crange[2 * k + 1] - crange[2 * k];
       const long long n32 = crange[2 * (CQG_NQC + k) + 1] - crange[2 * (CQG_NQC + k)];
       if (n64 > 0) ctx->launches += 1;
@@ -884,9 +955,14 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
       CUCHK(cudaStreamSynchronize(st));
       for (int k = 0; k < CQG_NQC; ++k) {
         float ms = 0.f;
-        if (cudaEventElapsedTime(&ms, ctx->ev[4 + 2 * k], ctx->ev[5 + 2 * k]) == cudaSuccess)
+        if (!class_fused(ctx->fused_tier, k) &&
+            cudaEventElapsedTime(&ms, ctx->ev[4 + 2 * k], ctx->ev[5 + 2 * k]) == cudaSuccess)
           ctx->stats.class_ms[k] += ms;
       }
+      float ms = 0.f;
+      if (ctx->fused_tier &&
+          cudaEventElapsedTime(&ms, ctx->ev[4 + 2 * CQG_NQC], ctx->ev[5 + 2 * CQG_NQC]) == cudaSuccess)
+        ctx->stats.ms_fused += ms;
     }
     first_chunk = false;
   }
@@ -1291,6 +1367,24 @@ cqg_status cqg_get_schedule(cqg_ctx *ctx, int *cta_per_sm, int *warps_per_cta, i
   return CQG_OK;
 }
 
+cqg_status cqg_set_fusion(cqg_ctx *ctx, int tier) {
+  if (!ctx) return CQG_ERR_BAD_ARG;
+  if (tier < 0 || tier > 2) {
+    ctx->err = "cqg_set_fusion: tier is 0 (per-class launches), 1 or 2";
+    return CQG_ERR_BAD_ARG;
+  }
+  ctx->fused_tier = tier;
+  return CQG_OK;
+}
+
+cqg_status cqg_get_fusion(cqg_ctx *ctx, int *tier, double *tuned_ms) {
+  if (!ctx) return CQG_ERR_BAD_ARG;
+  if (tier) *tier = ctx->fused_tier;
+  if (tuned_ms)
+    for (int t = 0; t < 3; ++t) tuned_ms[t] = ctx->fusion_ms[t];
+  return CQG_OK;
+}
+
 cqg_status cqg_set_schedule(cqg_ctx *ctx, const int *cta_per_sm, const int *warps_per_cta,
                             const int *quartets_per_warp, const int *warp_form) {
   if (!ctx) return CQG_ERR_BAD_ARG;
@@ -1325,7 +1419,7 @@ cqg_status cqg_get_stats(cqg_ctx *ctx, cqg_stats *out) {
     float ms;
     cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
     s.ms_screen = ms;
-    double eri = 0.0;
+    double eri = s.ms_fused;
     for (int k = 0; k < CQG_NQC; ++k) eri += s.class_ms[k];
     s.ms_eri = eri;
     cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[3]);

@@ -1154,6 +1154,10 @@ struct cqg_ctx {
   int shape_qpw[2 * CQG_NQC] = {0};
   // kernel form of a list whose class has both: 0 = per-thread (default), 1 = warp-cooperative
   int shape_var[2 * CQG_NQC] = {0};
+  // 0: one launch per class list; 1 or 2: the lists of that tier's classes go through one
+  // class-fused persistent kernel (eri_fused.cu); set by the autotuner or cqg_set_fusion
+  int fused_tier = 0;
+  double fusion_ms[3] = {0.0, 0.0, 0.0};   // autotuner's times of the three forms (ms)
   DevBuf<unsigned long long> d_qhead;  // work-queue head counter of every (precision, class) list
   int autotune_pending = 0;
   long long graph_capacity = 0;        // > 0: sync-free contraction for CUDA-graph capture
@@ -1202,7 +1206,7 @@ struct cqg_ctx {
   DevBuf<double> d_G, d_X, d_AX, d_Gscratch;
   BlockTable bt;
   int ntask = 0;
-  cudaEvent_t ev[4 + 2 * 55];
+  cudaEvent_t ev[4 + 2 * 55 + 2];
   bool events = false;
   cqg_stats stats;
   double *oe_table = nullptr;   // device address of the fixed charge table (cqg_one_e_noalloc)
@@ -1303,6 +1307,12 @@ static inline Mols make_mols(cqg_ctx *ctx) {
 }
 
 typedef cudaError_t (*eri_launcher)(cqg_ctx *, int blk, long long n, cudaStream_t st, const DigestGroups &dg);
+
+// Class-fused schedule (eri_fused.cu): whether class (la lb|lc ld) belongs to the fused
+// kernel of `tier` (1: (ss|ss) and (ps|ss), 2: every per-thread class up to (dd|dd)), and one
+// launch of that kernel over the current list ranges.
+bool cqg_fused_member(int tier, int la, int lb, int lc, int ld);
+cudaError_t cqg_launch_fused(cqg_ctx *ctx, int tier, cudaStream_t st, const DigestGroups &dg);
 
 template <int LA, int LB, int LC, int LD, typename T>
 static cudaError_t launch_eri(cqg_ctx *ctx, int blk, long long n, cudaStream_t st, const DigestGroups &dg) {

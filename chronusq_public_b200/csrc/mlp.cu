@@ -19,7 +19,7 @@
 
 namespace {
 
-constexpr int GM = 128, GN = 128, GK = 32, GKP = GK + 8;   // block tile; padded smem rows
+constexpr int GM = 128, GN = 128, GK = 32, GKP = GK + 8;   // large block tile; padded smem rows
 
 __device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
 __device__ __forceinline__ float silu_grad(float z) {
@@ -43,13 +43,14 @@ __device__ __forceinline__ void mma_16816(float (&d)[4], const uint32_t (&a)[4],
 // Stage rows [r0, r0 + 128) x k [k0, k0 + 32) of X(r, k) = X[r * sr + k * sk] into S[row][k]
 // (zero outside nrows x K).  Rows or k contiguous and 16-byte aligned: 8-element vector
 // loads; anything else element by element.
+template <int ROWS>
 __device__ __forceinline__ void stage_tile(const __nv_bfloat16 *__restrict__ X, long long sr, long long sk, int r0,
                                            int nrows, int k0, int K, bool vec_k, bool vec_r,
                                            __nv_bfloat16 (*S)[GKP]) {
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, nth = blockDim.x;
   const __nv_bfloat16 zero = __float2bfloat16(0.f);
   if (vec_k) {                 // sk == 1, sr % 8 == 0, K % 8 == 0, X 16-byte aligned
-    for (int e = tid; e < 128 * (GK / 8); e += 256) {
+    for (int e = tid; e < ROWS * (GK / 8); e += nth) {
       const int rr = e / (GK / 8), kv = (e % (GK / 8)) * 8;
       const int r = r0 + rr, k = k0 + kv;
       uint4 v = make_uint4(0, 0, 0, 0);
@@ -57,8 +58,8 @@ __device__ __forceinline__ void stage_tile(const __nv_bfloat16 *__restrict__ X, 
       *reinterpret_cast<uint4 *>(&S[rr][kv]) = v;
     }
   } else if (vec_r) {          // sr == 1, sk % 8 == 0, nrows % 8 == 0, X 16-byte aligned
-    for (int e = tid; e < GK * 16; e += 256) {
-      const int kk = e / 16, rv = (e % 16) * 8;
+    for (int e = tid; e < GK * (ROWS / 8); e += nth) {
+      const int kk = e / (ROWS / 8), rv = (e % (ROWS / 8)) * 8;
       const int r = r0 + rv, k = k0 + kk;
       uint4 v = make_uint4(0, 0, 0, 0);
       if (r < nrows && k < K) v = *reinterpret_cast<const uint4 *>(X + r + (long long)k * sk);
@@ -67,52 +68,55 @@ __device__ __forceinline__ void stage_tile(const __nv_bfloat16 *__restrict__ X, 
       for (int i = 0; i < 8; ++i) S[rv + i][kk] = h[i];
     }
   } else if (sk <= sr) {       // k varies fastest across threads
-    for (int e = tid; e < 128 * GK; e += 256) {
+    for (int e = tid; e < ROWS * GK; e += nth) {
       const int rr = e / GK, kk = e % GK;
       const int r = r0 + rr, k = k0 + kk;
       S[rr][kk] = (r < nrows && k < K) ? X[(long long)r * sr + (long long)k * sk] : zero;
     }
   } else {                     // rows vary fastest across threads
-    for (int e = tid; e < 128 * GK; e += 256) {
-      const int kk = e / 128, rr = e % 128;
+    for (int e = tid; e < ROWS * GK; e += nth) {
+      const int kk = e / ROWS, rr = e % ROWS;
       const int r = r0 + rr, k = k0 + kk;
       S[rr][kk] = (r < nrows && k < K) ? X[(long long)r * sr + (long long)k * sk] : zero;
     }
   }
 }
 
-// 256 threads = 8 warps; warp w computes rows (w % 4) * 32 .. +32 and columns (w / 4) * 64
-// .. +64 of the block's 128 x 128 tile: 2 x 8 tensor-core tiles per 16-wide k step.
-__global__ void __launch_bounds__(256) k_gemm_bf16(const __nv_bfloat16 *__restrict__ A, long long sam, long long sak,
-                                                   const __nv_bfloat16 *__restrict__ B, long long sbn, long long sbk,
-                                                   float *__restrict__ C, long long ldc, int M, int N, int K,
-                                                   const float *__restrict__ bias, __nv_bfloat16 *__restrict__ Y,
-                                                   long long ldy, int act, int accumulate) {
-  __shared__ __align__(16) __nv_bfloat16 As[GM][GKP];
-  __shared__ __align__(16) __nv_bfloat16 Bs[GN][GKP];
+// Block tile BM x BN (BM, BN multiples of 32), warps of 32 x WN output each (WN = 64 or 32):
+// (BM / 32) x (BN / WN) warps; per 16-wide k step a warp issues 2 x (WN / 8) tensor-core
+// tiles.  128 x 128 with 8 warps of 32 x 64 for large problems, 64 x 64 with 4 warps of
+// 32 x 32 when the large tiles would leave most of the 148 SMs idle.
+template <int BM, int BN, int WN>
+__global__ void __launch_bounds__((BM / 32) * (BN / WN) * 32)
+    k_gemm_bf16(const __nv_bfloat16 *__restrict__ A, long long sam, long long sak, const __nv_bfloat16 *__restrict__ B,
+                long long sbn, long long sbk, float *__restrict__ C, long long ldc, int M, int N, int K,
+                const float *__restrict__ bias, __nv_bfloat16 *__restrict__ Y, long long ldy, int act, int accumulate) {
+  constexpr int NWM = BM / 32, NJ = WN / 8;
+  __shared__ __align__(16) __nv_bfloat16 As[BM][GKP];
+  __shared__ __align__(16) __nv_bfloat16 Bs[BN][GKP];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int wm = (warp & 3) * 32, wn = (warp >> 2) * 64;
-  const int m0 = blockIdx.y * GM, n0 = blockIdx.x * GN;
+  const int wm = (warp % NWM) * 32, wn = (warp / NWM) * WN;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
   const int g = lane >> 2, t = lane & 3;
   const bool a16 = (reinterpret_cast<uintptr_t>(A) & 15) == 0, b16 = (reinterpret_cast<uintptr_t>(B) & 15) == 0;
   const bool avk = a16 && sak == 1 && sam % 8 == 0 && K % 8 == 0;
   const bool avr = a16 && !avk && sam == 1 && sak % 8 == 0 && M % 8 == 0;
   const bool bvk = b16 && sbk == 1 && sbn % 8 == 0 && K % 8 == 0;
   const bool bvr = b16 && !bvk && sbn == 1 && sbk % 8 == 0 && N % 8 == 0;
-  float acc[2][8][4];
+  float acc[2][NJ][4];
 #pragma unroll
   for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 8; ++j)
+    for (int j = 0; j < NJ; ++j)
 #pragma unroll
       for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
   for (int k0 = 0; k0 < K; k0 += GK) {
-    stage_tile(A, sam, sak, m0, M, k0, K, avk, avr, As);
-    stage_tile(B, sbn, sbk, n0, N, k0, K, bvk, bvr, Bs);
+    stage_tile<BM>(A, sam, sak, m0, M, k0, K, avk, avr, As);
+    stage_tile<BN>(B, sbn, sbk, n0, N, k0, K, bvk, bvr, Bs);
     __syncthreads();
 #pragma unroll
     for (int ks = 0; ks < GK; ks += 16) {
-      uint32_t af[2][4], bf[8][2];
+      uint32_t af[2][4], bf[NJ][2];
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
         const int r = wm + i * 16 + g;
@@ -122,7 +126,7 @@ __global__ void __launch_bounds__(256) k_gemm_bf16(const __nv_bfloat16 *__restri
         af[i][3] = *reinterpret_cast<const uint32_t *>(&As[r + 8][ks + 2 * t + 8]);
       }
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
+      for (int j = 0; j < NJ; ++j) {
         const int c = wn + j * 8 + g;
         bf[j][0] = *reinterpret_cast<const uint32_t *>(&Bs[c][ks + 2 * t]);
         bf[j][1] = *reinterpret_cast<const uint32_t *>(&Bs[c][ks + 2 * t + 8]);
@@ -130,14 +134,14 @@ __global__ void __launch_bounds__(256) k_gemm_bf16(const __nv_bfloat16 *__restri
 #pragma unroll
       for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) mma_16816(acc[i][j], af[i], bf[j]);
+        for (int j = 0; j < NJ; ++j) mma_16816(acc[i][j], af[i], bf[j]);
     }
     __syncthreads();
   }
 #pragma unroll
   for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 8; ++j)
+    for (int j = 0; j < NJ; ++j)
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const int m = m0 + wm + i * 16 + g + (q >> 1) * 8, n = n0 + wn + j * 8 + 2 * t + (q & 1);
@@ -204,6 +208,24 @@ __global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float
   if (wbf) wbf[i] = __float2bfloat16(w[i]);
 }
 
+// The same step with the learning rate and the two bias corrections read from device memory
+// (hyper = {lr, 1 - b1^step, 1 - b2^step}), so that a captured training step can be replayed
+// with a schedule that changes from step to step.
+__global__ void k_adam_dev(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m1,
+                           float *__restrict__ m2, long long n, const float *__restrict__ hyper, float b1, float b2,
+                           float eps, float wd, __nv_bfloat16 *__restrict__ wbf) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float lr = hyper[0], bc1 = hyper[1], bc2 = hyper[2];
+  const float gi = g[i] + wd * w[i];
+  const float a = b1 * m1[i] + (1.f - b1) * gi;
+  const float b = b2 * m2[i] + (1.f - b2) * gi * gi;
+  m1[i] = a;
+  m2[i] = b;
+  w[i] -= lr * (a / bc1) / (sqrtf(b / bc2) + eps);
+  if (wbf) wbf[i] = __float2bfloat16(w[i]);
+}
+
 inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
@@ -215,11 +237,20 @@ cqg_status cqg_mlp_gemm_bf16(const void *A, long long sam, long long sak, const 
                              int act, int accumulate, void *stream) {
   if (!A || !B || !C || M < 0 || N < 0 || K < 0) return CQG_ERR_BAD_ARG;
   if (M == 0 || N == 0) return CQG_OK;
-  if ((M + GM - 1) / GM > 65535) return CQG_ERR_BAD_ARG;   // grid.y limit: M <= 8.4 M rows
-  dim3 grid((N + GN - 1) / GN, (M + GM - 1) / GM);
-  k_gemm_bf16<<<grid, 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)A, sam, sak, (const __nv_bfloat16 *)B,
-                                                      sbn, sbk, C, ldc, M, N, K, bias, (__nv_bfloat16 *)Y, ldy, act,
-                                                      accumulate);
+  const long long big_blocks = (long long)((N + GN - 1) / GN) * ((M + GM - 1) / GM);
+  cudaStream_t st = (cudaStream_t)stream;
+  const __nv_bfloat16 *a = (const __nv_bfloat16 *)A, *b = (const __nv_bfloat16 *)B;
+  if (big_blocks >= 296) {   // two waves of 148 SMs or more: large tiles
+    if ((M + GM - 1) / GM > 65535) return CQG_ERR_BAD_ARG;   // grid.y limit
+    dim3 grid((N + GN - 1) / GN, (M + GM - 1) / GM);
+    k_gemm_bf16<GM, GN, 64><<<grid, 256, 0, st>>>(a, sam, sak, b, sbn, sbk, C, ldc, M, N, K, bias,
+                                                  (__nv_bfloat16 *)Y, ldy, act, accumulate);
+  } else {
+    if ((M + 63) / 64 > 65535) return CQG_ERR_BAD_ARG;
+    dim3 grid((N + 63) / 64, (M + 63) / 64);
+    k_gemm_bf16<64, 64, 32><<<grid, 128, 0, st>>>(a, sam, sak, b, sbn, sbk, C, ldc, M, N, K, bias,
+                                                  (__nv_bfloat16 *)Y, ldy, act, accumulate);
+  }
   return cudaGetLastError() == cudaSuccess ? CQG_OK : CQG_ERR_CUDA;
 }
 
@@ -254,6 +285,14 @@ cqg_status cqg_mlp_adam(float *w, const float *g, float *m1, float *m2, long lon
   const float bc1 = 1.f - powf(b1, (float)step), bc2 = 1.f - powf(b2, (float)step);
   k_adam<<<nblk(n, 256), 256, 0, (cudaStream_t)stream>>>(w, g, m1, m2, n, lr, b1, b2, eps, bc1, bc2, weight_decay,
                                                          (__nv_bfloat16 *)wbf);
+  return cudaGetLastError() == cudaSuccess ? CQG_OK : CQG_ERR_CUDA;
+}
+
+cqg_status cqg_mlp_adam_dev(float *w, const float *g, float *m1, float *m2, long long n, const float *hyper,
+                            float b1, float b2, float eps, float weight_decay, void *wbf, void *stream) {
+  if (n <= 0 || !hyper) return CQG_ERR_BAD_ARG;
+  k_adam_dev<<<nblk(n, 256), 256, 0, (cudaStream_t)stream>>>(w, g, m1, m2, n, hyper, b1, b2, eps, weight_decay,
+                                                             (__nv_bfloat16 *)wbf);
   return cudaGetLastError() == cudaSuccess ? CQG_OK : CQG_ERR_CUDA;
 }
 

@@ -371,10 +371,29 @@ class PairMLP:
         Xn = (np.asarray(X) - self.xmean) / self.xstd
         return t.tensor(Xn, dtype=t.float32, device=self.dev).to(t.bfloat16).contiguous()
 
-    def fit(self, X, T, M, epochs: int = 40, batch: int = 2048, lr: float = 2e-3, seed: int = 0, log=None):
+    def adam_dev(self, gW, gb, hyper, wd: float = 0.0):
+        """Adam step with {lr, 1 - b1^step, 1 - b2^step} read from the device tensor `hyper`
+        (capturable in a CUDA graph); the host step counter advances as in :meth:`adam`."""
+        self.step += 1
+        for i in range(len(self.W)):
+            _lib.check(self.L.cqg_mlp_adam_dev(self._p(self.W[i]), self._p(gW[i]), self._p(self.mW[i]),
+                                               self._p(self.vW[i]), self.W[i].numel(), self._p(hyper), 0.9, 0.999,
+                                               1e-8, wd, self._p(self.Wbf[i]), self._stream()))
+            _lib.check(self.L.cqg_mlp_adam_dev(self._p(self.b[i]), self._p(gb[i]), self._p(self.mb[i]),
+                                               self._p(self.vb[i]), self.b[i].numel(), self._p(hyper), 0.9, 0.999,
+                                               1e-8, 0.0, None, self._stream()))
+
+    def fit(self, X, T, M, epochs: int = 40, batch: int = 2048, lr: float = 2e-3, seed: int = 0, log=None,
+            graph: bool = True):
         """Masked-MSE training on (features, local-frame targets, masks).  Inputs are
         standardised per feature, targets by their masked mean per output and one global
-        scale.  Returns the per-epoch mean training loss (standardised units)."""
+        scale.  Returns the per-epoch mean training loss (standardised units).
+
+        With `graph`, one full-batch training step (batch gather, forward, loss, backward,
+        Adam with the step's learning rate and bias corrections taken from device memory)
+        is captured once as a CUDA graph and replayed for every later full batch; the
+        partial last batch of an epoch runs uncaptured.  The arithmetic is the same as the
+        uncaptured loop's."""
         t = self.torch
         X = np.asarray(X)
         T = np.asarray(T)
@@ -392,20 +411,56 @@ class PairMLP:
         g = t.Generator(device=self.dev)
         g.manual_seed(seed)
         hist = []
-        steps = max(1, epochs * ((n + batch - 1) // batch))
+        per_epoch = (n + batch - 1) // batch
+        steps = max(1, epochs * per_epoch)
+
+        def lr_at(k):
+            warm = min(1.0, (k + 1) / 100.0)
+            return lr * warm * 0.5 * (1.0 + math.cos(math.pi * k / steps))
+
+        # {lr, 1 - b1^step, 1 - b2^step} of every step, on the device
+        sched = np.array([[lr_at(k), 1.0 - 0.9 ** (self.step + k + 1), 1.0 - 0.999 ** (self.step + k + 1)]
+                          for k in range(steps)], dtype=np.float32)
+        sched_d = t.tensor(sched, device=self.dev)
+        hyper = t.zeros(3, dtype=t.float32, device=self.dev)
+        idx_s = t.zeros(batch, dtype=t.int64, device=self.dev)
+        tot = t.zeros(1, dtype=t.float32, device=self.dev)
+        use_graph = graph and n >= 2 * batch
+        stream = t.cuda.Stream(device=self.dev) if use_graph else None
+        cuda_graph = None
+
+        def step_body(idx, nb):
+            out, cache = self.forward(Xd.index_select(0, idx), keep=True)
+            loss, dout = self.loss_grad(out, Td.index_select(0, idx), Md.index_select(0, idx), 1.0 / float(nb))
+            gW, gb = self.backward(dout, cache)
+            self.adam_dev(gW, gb, hyper)
+            tot.add_(loss * nb)
+
         k = 0
         for ep in range(epochs):
             perm = t.randperm(n, device=self.dev, generator=g)
-            tot = t.zeros(1, dtype=t.float32, device=self.dev)
+            tot.zero_()
             for s in range(0, n, batch):
                 idx = perm[s:s + batch]
-                out, cache = self.forward(Xd[idx].contiguous(), keep=True)
-                loss, dout = self.loss_grad(out, Td[idx].contiguous(), Md[idx].contiguous(),
-                                            1.0 / float(idx.numel()))
-                gW, gb = self.backward(dout, cache)
-                warm = min(1.0, (k + 1) / 100.0)
-                self.adam(gW, gb, lr=lr * warm * 0.5 * (1.0 + math.cos(math.pi * k / steps)))
-                tot += loss * idx.numel()
+                nb = int(idx.numel())
+                hyper.copy_(sched_d[k])
+                if nb == batch and cuda_graph is not None:
+                    idx_s.copy_(idx)
+                    cuda_graph.replay()
+                    self.step += 1                    # the captured Adam's step, on the host
+                else:
+                    step_body(idx, nb)
+                    if use_graph and cuda_graph is None and nb == batch:
+                        # capture the full-batch step once (after this eager one warmed it up)
+                        t.cuda.synchronize(self.dev)
+                        cuda_graph = t.cuda.CUDAGraph()
+                        stream.wait_stream(t.cuda.current_stream(self.dev))
+                        step0 = self.step
+                        with t.cuda.stream(stream):
+                            with t.cuda.graph(cuda_graph, stream=stream):
+                                step_body(idx_s, batch)
+                        t.cuda.current_stream(self.dev).wait_stream(stream)
+                        self.step = step0                 # capture enqueued nothing
                 k += 1
             hist.append(float(tot) / n)
             if log:

@@ -63,6 +63,8 @@ typedef struct {
   long long chunks;                /* quartet-list chunks the call was processed in */
   long long class_quartets[55];    /* per quartet class (index: see cqg_class_name) */
   double class_ms[55];             /* device time per class kernel (ms), if timing on */
+  double ms_fused;                 /* device time of the class-fused kernel (ms), if timing on */
+  int fused_tier;                  /* 0: per-class launches; 1, 2: class-fused tier used */
 } cqg_stats;
 
 /* Library / context lifetime. */
@@ -203,6 +205,16 @@ cqg_status cqg_get_launch_shapes(cqg_ctx *ctx, int *cta_per_sm, int *warps_per_c
  * first three = default. */
 cqg_status cqg_get_schedule(cqg_ctx *ctx, int *cta_per_sm, int *warps_per_cta, int *quartets_per_warp,
                             int *warp_form);
+/* Class fusion: tier 0 launches one kernel per class list; tier 1 evaluates the lists of
+ * (ss|ss) and (ps|ss), tier 2 those of every
+ * per-thread class up to (dd|dd), FP64 and FP32 alike, in one persistent kernel that pulls
+ * chunks of every list from one device work queue; the other classes keep their own
+ * launches.  The autotuner (cqg_autotune_next) times the three forms and keeps the fastest;
+ * cqg_get_fusion returns the tier in use and the autotuner's times of tiers 0, 1, 2 (ms;
+ * zero before tuning).  No reference counterpart (the reference's loop is one OpenMP
+ * round-robin over all quartets, aointegrals_contract.h:107). */
+cqg_status cqg_set_fusion(cqg_ctx *ctx, int tier);
+cqg_status cqg_get_fusion(cqg_ctx *ctx, int *tier, double *tuned_ms);
 /* Set the schedule of every list from arrays laid out as cqg_get_schedule's (NULL leaves
  * that part unchanged; the kernel form is taken only for classes that have both forms):
  * a schedule tuned once can be given to other contexts of the same system.  Entries out of
@@ -242,6 +254,12 @@ cqg_status cqg_mlp_mse(const float *pred, const float *target, const float *mask
 cqg_status cqg_mlp_adam(float *w, const float *g, float *m1, float *m2, long long n, float lr,
                         float b1, float b2, float eps, int step, float weight_decay, void *wbf,
                         void *stream);
+/* cqg_mlp_adam with the learning rate and the bias corrections read on the device from
+ * hyper = {lr, 1 - b1^step, 1 - b2^step} (device pointer): the call can be captured in a
+ * CUDA graph and replayed with a per-step schedule. */
+cqg_status cqg_mlp_adam_dev(float *w, const float *g, float *m1, float *m2, long long n,
+                            const float *hyper, float b1, float b2, float eps, float weight_decay,
+                            void *wbf, void *stream);
 
 /* FP64 / FP32 FMA throughput probe used to report roofline fractions: runs a dependent
  * FMA chain kernel for `ms_target` ms and returns achieved TFLOP/s in *tflops. */

@@ -18,7 +18,8 @@ def _p(x):
 
 
 @pytest.mark.parametrize("M,N,K,trans_a,epilogue", [(300, 196, 57, False, True), (256, 256, 256, True, False),
-                                                     (17, 5, 33, False, True), (64, 64, 1000, True, True)])
+                                                     (17, 5, 33, False, True), (64, 64, 1000, True, True),
+                                                     (20000, 256, 256, False, True), (20000, 196, 64, True, False)])
 def test_gemm_bf16_matches_torch_fp32(M, N, K, trans_a, epilogue):
     import torch
     L = _lib.lib()
@@ -176,3 +177,26 @@ def test_projected_learned_guess_in_a_larger_basis():
             assert hf.guess_used == "LEARNED"
         hf.close()
     assert abs(Es[0] - Es[1]) < 1e-8
+
+
+def test_graph_captured_training_matches_uncaptured():
+    """fit() with the training step captured as a CUDA graph takes the same steps as the
+    uncaptured loop: same weights (the step has no order-dependent reductions) and loss
+    history within FP32 rounding of the loss sum."""
+    import torch
+    from chronusq_public_b200.guess_model import PairMLP, NFEAT, MAXF
+    rng = np.random.default_rng(5)
+    n = 5000
+    X = rng.normal(size=(n, NFEAT)).astype(np.float32)
+    X[:, -1] = 1.0
+    T = rng.normal(size=(n, MAXF * MAXF)).astype(np.float32)
+    M = (rng.uniform(size=T.shape) < 0.7).astype(np.float32)
+    a = PairMLP(width=64, layers=2, seed=9)
+    b = PairMLP(width=64, layers=2, seed=9)
+    ha = a.fit(X, T, M, epochs=3, batch=512, graph=True)
+    hb = b.fit(X, T, M, epochs=3, batch=512, graph=False)
+    torch.cuda.synchronize()
+    assert a.step == b.step
+    for wa, wb in zip(a.W + a.b, b.W + b.b):
+        assert (wa - wb).abs().max().item() <= 1e-6
+    assert np.allclose(ha, hb, rtol=1e-4)

@@ -15,15 +15,18 @@ def _rand_density(n, seed):
     return np.asfortranarray(0.5 * (a + a.T))
 
 
-@pytest.mark.parametrize("cutoff,warp_form", [(1e-10, 0), (1e-8, 0), (1e-6, 0), (1e-6, 1)])
-def test_mixed_G_close_to_fp64(cutoff, warp_form):
+@pytest.mark.parametrize("cutoff,warp_form,tier", [(1e-10, 0, 0), (1e-8, 0, 0), (1e-6, 0, 0), (1e-6, 1, 0),
+                                                   (1e-6, 0, 2)])
+def test_mixed_G_close_to_fp64(cutoff, warp_form, tier):
     """warp_form = 1: the classes with both kernel forms run their FP64 and FP32 lists in
-    the warp-cooperative form."""
+    the warp-cooperative form; tier 2: the per-thread classes' FP64 and FP32 lists go
+    through the class-fused kernel."""
     from chronusq_public_b200.aointegrals import AOIntegrals, PREC_MIXED, PREC_FP64
     mol = water_cluster(4, 21)
     bs = BasisSet("cc-pvdz", mol.atoms, mol.coords)
     ints = AOIntegrals(bs)
     ints.setSchedule(warp_form=warp_form)
+    ints.setFusion(tier)
     D = _rand_density(bs.nbasis, 4)
     G64, _ = ints.formPT(D)
     n64 = ints.stats()["quartets"]

@@ -245,3 +245,44 @@ def test_set_schedule_rejects_out_of_range_entries():
     assert e.value.status == 1
     assert ints.schedule() == before
     ints.close()
+
+
+@pytest.mark.parametrize("tier", [1, 2])
+def test_class_fused_kernel_matches_oracle(tier):
+    """The class-fused persistent kernel (one launch, one device work queue over the lists
+    of the tier's classes) gives the oracle's G and quartet count, RHF and UHF lists."""
+    mol = water_cluster(3, 11)
+    bs = BasisSet("cc-pvdz", mol.atoms, mol.coords)
+    ob = O.OracleBasis.from_basis(bs)
+    Ps = rand_sym(bs.nbasis, 51)
+    Pz = rand_sym(bs.nbasis, 52, 0.2)
+    ints = _aoi()(bs)
+    ints.setFusion(tier)
+    ints.setTiming(True)
+    PTs, PTz = ints.formPT(Ps, Pz)
+    st = ints.stats()
+    assert st["fused_tier"] == tier and st["ms_fused"] > 0.0
+    PTs_r, PTz_r, nr = O.form_pt(ob, Ps, Pz)
+    assert st["quartets"] == nr
+    assert np.abs(PTs - PTs_r).max() <= TOL_G
+    assert np.abs(PTz - PTz_r).max() <= TOL_G
+    G, _ = ints.formPT(Ps)
+    G_r, _, _ = O.form_pt(ob, Ps)
+    assert np.abs(G - G_r).max() <= TOL_G
+    ints.close()
+
+
+def test_autotuner_picks_a_fusion_tier_and_keeps_parity():
+    mol = water_cluster(3, 12)
+    bs = BasisSet("cc-pvdz", mol.atoms, mol.coords)
+    ob = O.OracleBasis.from_basis(bs)
+    D = rand_sym(bs.nbasis, 53)
+    ints = _aoi()(bs)
+    ints.autotune_next()
+    G1, _ = ints.formPT(D)
+    tier, ms = ints.fusion()
+    assert tier in (0, 1, 2) and all(t > 0.0 for t in ms)
+    G2, _ = ints.formPT(D)
+    Gr, _, _ = O.form_pt(ob, D)
+    assert np.abs(G1 - Gr).max() <= TOL_G and np.abs(G2 - Gr).max() <= TOL_G
+    ints.close()
