@@ -543,13 +543,17 @@ def main():
         peak64 = probe_fma_peak(True, 100.0, local)
         eri_s = sum(eri_ms) / len(eri_ms) * 1e-3
         achieved = (sum(mflops) / len(mflops)) / eri_s / 1e12
-        traffic = None
+        # DRAM bytes per build of the ERI kernels: the per-quartet figure of an ncu capture of
+        # this workload (SAD density, autotuned schedule; profiles/traffic.json) times this
+        # step's quartets; null for a workload or density that was not captured
+        traffic, traffic_src = None, "no ncu capture of this workload"
         tj = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tj):
+        if os.path.exists(tj) and args.density == "sad":
             try:
                 tr = json.load(open(tj)).get(args.workload)
                 if tr:
                     traffic = tr["bytes_per_quartet"] * quartets[0]
+                    traffic_src = tr.get("source", "profiles/traffic.json")
             except (ValueError, KeyError):
                 traffic = None
         line = {
@@ -565,7 +569,7 @@ def main():
                          "peak_source": "measured: FP64 FMA-chain probe (cqg_probe_fma_peak) on this GPU",
                          "flop_model": "MD-v1 (model FLOPs of the screened quartets)",
                          "model_flops_per_step": mflops[0], "eri_ms_per_step": eri_s * 1e3,
-                         "traffic": traffic},
+                         "traffic": traffic, "traffic_source": traffic_src},
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "schedule": schedule_summary(ints, st_last),
