@@ -21,6 +21,43 @@ from .batch import BatchAOIntegrals
 from .molecule import Molecule
 
 
+def occupied_projector(F, nocc: int, max_iter: int = 100, check: int = 4, finish: int = 3):
+    """Projector on the `nocc` lowest eigenvectors of each symmetric matrix of the stack F
+    (..., n, n), by trace-correcting purification (A. M. N. Niklasson, Phys. Rev. B 66,
+    155115 (2002)): the Gershgorin interval [lo, hi] of each matrix is mapped onto [0, 1],
+    X0 = (hi I - F) / (hi - lo), so the lowest orbitals sit nearest 1; each step replaces X
+    by X^2 or by 2X - X^2, whichever brings the trace nearer nocc, which drives every
+    eigenvalue to 0 or 1 with the trace held at nocc.  Once every matrix has
+    tr X - tr X^2 < 1e-6 (each eigenvalue within about 1e-6 of 0 or 1) and its trace within
+    1e-3 of nocc, `finish` more steps take the deviations, which square at every step, to
+    the rounding floor.  The convergence is read back every `check` steps.  Returns None
+    when that is not reached in `max_iter` steps (no gap at the Fermi level): the caller
+    diagonalises.  Everything is batched FP64 matrix products on the device."""
+    import torch as t
+    n = F.shape[-1]
+    diag = F.diagonal(dim1=-2, dim2=-1)
+    rad = F.abs().sum(-1) - diag.abs()
+    lo = (diag - rad).amin(-1)
+    hi = (diag + rad).amax(-1)
+    eye = t.eye(n, dtype=F.dtype, device=F.device)
+    X = (hi[..., None, None] * eye - F) / (hi - lo).clamp_min(1e-300)[..., None, None]
+    left = None
+    for it in range(1, max_iter + 1):
+        X2 = X @ X
+        tr1 = X.diagonal(dim1=-2, dim2=-1).sum(-1)
+        tr2 = X2.diagonal(dim1=-2, dim2=-1).sum(-1)
+        square = (tr2 - nocc).abs() <= (2.0 * tr1 - tr2 - nocc).abs()
+        X = t.where(square[..., None, None], X2, 2.0 * X - X2)
+        if left is not None:
+            left -= 1
+            if left == 0:
+                return 0.5 * (X + X.transpose(-1, -2))
+        elif it % check == 0:
+            if float((tr1 - tr2).abs().max()) < 1e-6 and float((tr1 - nocc).abs().max()) < 1e-3:
+                left = finish
+    return None
+
+
 class BatchSCF:
     def __init__(self, molecules: Sequence[Molecule], basis: str, device: int = 0,
                  thresholdSchwartz: float = 1e-12, ndiis: int = 6):
@@ -32,6 +69,7 @@ class BatchSCF:
         self.dev = torch.device("cuda", device)
         self.B = BatchAOIntegrals(self.bss, device=device, thresholdSchwartz=thresholdSchwartz)
         self.thresh = thresholdSchwartz
+        self.density_method = "purify"     # or "eigh": see _density
         self.nmol = len(self.mols)
         self.nocc = []
         for m in self.mols:
@@ -75,11 +113,18 @@ class BatchSCF:
 
     # ------------------------------------------------------------------ pieces ---
     def _density(self, FO, g):
+        """AO density 2 X Q X^T of a stack of orthonormal Fock matrices, Q the projector on the
+        nocc lowest orbitals: by purification (`density_method` "purify", batched GEMMs) or
+        by eigenvectors ("eigh"); the same aufbau density when the HOMO-LUMO gap is open."""
         t = self.torch
-        _, C = t.linalg.eigh(0.5 * FO)
-        Co = C[..., : g["nocc"]]
-        DO = 2.0 * Co @ Co.transpose(-1, -2)
-        return g["X"] @ DO @ g["X"].transpose(-1, -2)
+        Q = None
+        if self.density_method == "purify":
+            Q = occupied_projector(FO, g["nocc"])
+        if Q is None:
+            _, C = t.linalg.eigh(0.5 * FO)
+            Co = C[..., : g["nocc"]]
+            Q = Co @ Co.transpose(-1, -2)
+        return g["X"] @ (2.0 * Q) @ g["X"].transpose(-1, -2)
 
     def sad_density(self):
         from .scf import atomic_density

@@ -15,6 +15,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "../../include/cqgpu.h"
 
 namespace {
@@ -90,7 +92,8 @@ template <int BM, int BN, int WN>
 __global__ void __launch_bounds__((BM / 32) * (BN / WN) * 32)
     k_gemm_bf16(const __nv_bfloat16 *__restrict__ A, long long sam, long long sak, const __nv_bfloat16 *__restrict__ B,
                 long long sbn, long long sbk, float *__restrict__ C, long long ldc, int M, int N, int K,
-                const float *__restrict__ bias, __nv_bfloat16 *__restrict__ Y, long long ldy, int act, int accumulate) {
+                const float *__restrict__ bias, __nv_bfloat16 *__restrict__ Y, long long ldy, int act, int accumulate,
+                int kchunk) {
   constexpr int NWM = BM / 32, NJ = WN / 8;
   __shared__ __align__(16) __nv_bfloat16 As[BM][GKP];
   __shared__ __align__(16) __nv_bfloat16 Bs[BN][GKP];
@@ -110,9 +113,12 @@ __global__ void __launch_bounds__((BM / 32) * (BN / WN) * 32)
     for (int j = 0; j < NJ; ++j)
 #pragma unroll
       for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
-  for (int k0 = 0; k0 < K; k0 += GK) {
-    stage_tile<BM>(A, sam, sak, m0, M, k0, K, avk, avr, As);
-    stage_tile<BN>(B, sbn, sbk, n0, N, k0, K, bvk, bvr, Bs);
+  // split K (kchunk > 0): this block reduces k in [kb, ke) and adds its partial tile to C
+  // with atomics (C zeroed by the caller); no epilogue then
+  const int kb = kchunk > 0 ? blockIdx.z * kchunk : 0, ke = kchunk > 0 ? min(K, kb + kchunk) : K;
+  for (int k0 = kb; k0 < ke; k0 += GK) {
+    stage_tile<BM>(A, sam, sak, m0, M, k0, ke, avk, avr, As);
+    stage_tile<BN>(B, sbn, sbk, n0, N, k0, ke, bvk, bvr, Bs);
     __syncthreads();
 #pragma unroll
     for (int ks = 0; ks < GK; ks += 16) {
@@ -146,6 +152,10 @@ __global__ void __launch_bounds__((BM / 32) * (BN / WN) * 32)
       for (int q = 0; q < 4; ++q) {
         const int m = m0 + wm + i * 16 + g + (q >> 1) * 8, n = n0 + wn + j * 8 + 2 * t + (q & 1);
         if (m >= M || n >= N) continue;
+        if (kchunk > 0) {
+          atomicAdd(C + m * ldc + n, acc[i][j][q]);
+          continue;
+        }
         float z = acc[i][j][q] + (bias ? bias[n] : 0.f);
         if (accumulate) z += C[m * ldc + n];
         C[m * ldc + n] = z;
@@ -164,12 +174,26 @@ __global__ void k_to_bf16(const float *__restrict__ x, __nv_bfloat16 *__restrict
   if (i < n) y[i] = __float2bfloat16(x[i]);
 }
 
-__global__ void k_colsum(const __nv_bfloat16 *__restrict__ dZ, int M, int N, float *__restrict__ db) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
+// db[n] += sum over rows [blockIdx.y * 256, +256) of dZ[m][n]: 32 columns x 8 row groups
+// per block (a warp reads 32 consecutive columns of one row), partial sums reduced in shared
+// memory, one atomic per column and block (db zeroed by the caller).
+__global__ void __launch_bounds__(256) k_colsum(const __nv_bfloat16 *__restrict__ dZ, int M, int N,
+                                                float *__restrict__ db) {
+  __shared__ float part[8][33];
+  const int c = threadIdx.x & 31, rg = threadIdx.x >> 5;
+  const int n = blockIdx.x * 32 + c;
+  const int m0 = blockIdx.y * 256, m1 = min(M, m0 + 256);
   float s = 0.f;
-  for (int m = 0; m < M; ++m) s += __bfloat162float(dZ[(long long)m * N + n]);
-  db[n] = s;
+  if (n < N)
+    for (int m = m0 + rg; m < m1; m += 8) s += __bfloat162float(dZ[(long long)m * N + n]);
+  part[rg][c] = s;
+  __syncthreads();
+  if (rg == 0 && n < N) {
+    float t = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) t += part[k][c];
+    atomicAdd(db + n, t);
+  }
 }
 
 // loss = sum mask*(pred-target)^2 / count ; dpred = 2 mask (pred-target) / count
@@ -244,12 +268,27 @@ cqg_status cqg_mlp_gemm_bf16(const void *A, long long sam, long long sak, const 
     if ((M + GM - 1) / GM > 65535) return CQG_ERR_BAD_ARG;   // grid.y limit
     dim3 grid((N + GN - 1) / GN, (M + GM - 1) / GM);
     k_gemm_bf16<GM, GN, 64><<<grid, 256, 0, st>>>(a, sam, sak, b, sbn, sbk, C, ldc, M, N, K, bias,
-                                                  (__nv_bfloat16 *)Y, ldy, act, accumulate);
+                                                  (__nv_bfloat16 *)Y, ldy, act, accumulate, 0);
   } else {
     if ((M + 63) / 64 > 65535) return CQG_ERR_BAD_ARG;
-    dim3 grid((N + 63) / 64, (M + 63) / 64);
+    const long long tiles = (long long)((N + 63) / 64) * ((M + 63) / 64);
+    // few output tiles and a long reduction (weight gradients: K = batch rows): split K over
+    // blockIdx.z so that about two waves of CTAs run, partial tiles added with atomics
+    int splits = 1;
+    if (!bias && !Y && tiles < 148 && K >= 4 * GK) {
+      splits = (int)std::min<long long>((296 + tiles - 1) / tiles, K / (2 * GK));
+      splits = std::max(1, std::min(splits, 64));
+    }
+    const int kchunk = splits > 1 ? ((K + splits - 1) / splits + GK - 1) / GK * GK : 0;
+    if (kchunk > 0) {
+      splits = (K + kchunk - 1) / kchunk;
+      if (!accumulate) {
+        if (cudaMemset2DAsync(C, ldc * sizeof(float), 0, N * sizeof(float), M, st) != cudaSuccess) return CQG_ERR_CUDA;
+      }
+    }
+    dim3 grid((N + 63) / 64, (M + 63) / 64, splits);
     k_gemm_bf16<64, 64, 32><<<grid, 128, 0, st>>>(a, sam, sak, b, sbn, sbk, C, ldc, M, N, K, bias,
-                                                  (__nv_bfloat16 *)Y, ldy, act, accumulate);
+                                                  (__nv_bfloat16 *)Y, ldy, act, accumulate, kchunk);
   }
   return cudaGetLastError() == cudaSuccess ? CQG_OK : CQG_ERR_CUDA;
 }
@@ -268,7 +307,11 @@ cqg_status cqg_mlp_to_bf16(const float *x, void *y, long long n, void *stream) {
 
 cqg_status cqg_mlp_colsum(const void *dZ, int M, int N, float *db, void *stream) {
   if (N <= 0) return CQG_OK;
-  k_colsum<<<nblk(N, 128), 128, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)dZ, M, N, db);
+  if (cudaMemsetAsync(db, 0, (size_t)N * sizeof(float), (cudaStream_t)stream) != cudaSuccess) return CQG_ERR_CUDA;
+  if (M <= 0) return CQG_OK;
+  if ((M + 255) / 256 > 65535) return CQG_ERR_BAD_ARG;
+  dim3 grid((N + 31) / 32, (M + 255) / 256);
+  k_colsum<<<grid, 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)dZ, M, N, db);
   return cudaGetLastError() == cudaSuccess ? CQG_OK : CQG_ERR_CUDA;
 }
 

@@ -43,7 +43,8 @@ def batch_scf_comparison(count: int = 512, per_size: int = 2, basis: str = "6-31
     E = b.run(use_graph=True, autotune=True)
     sizes = [int(m.natoms // 3) for m in mols]
     res = {"molecules": count, "sizes_first": sizes[:8], "nbasis_total": int(sum(b.B.nbf)),
-           "batched_seconds": b.seconds, "batched_molecules_per_s": count / b.seconds,
+           "batched_seconds": b.seconds, "batched_fock_seconds": b.fock_seconds,
+           "batched_guess_seconds": b.guess_seconds, "batched_molecules_per_s": count / b.seconds,
            "batched_iterations_max": int(b.iterations.max()), "batched_fock_builds": b.fock_builds,
            "graph_replays": b.graph_replays, "graph_captures": b.graph_captures, "converged": bool(b.converged)}
     b.close()

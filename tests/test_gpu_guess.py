@@ -19,7 +19,8 @@ def _p(x):
 
 @pytest.mark.parametrize("M,N,K,trans_a,epilogue", [(300, 196, 57, False, True), (256, 256, 256, True, False),
                                                      (17, 5, 33, False, True), (64, 64, 1000, True, True),
-                                                     (20000, 256, 256, False, True), (20000, 196, 64, True, False)])
+                                                     (20000, 256, 256, False, True), (20000, 196, 64, True, False),
+                                                     (256, 196, 4096, True, False), (57, 256, 2000, True, False)])
 def test_gemm_bf16_matches_torch_fp32(M, N, K, trans_a, epilogue):
     import torch
     L = _lib.lib()
@@ -181,8 +182,8 @@ def test_projected_learned_guess_in_a_larger_basis():
 
 def test_graph_captured_training_matches_uncaptured():
     """fit() with the training step captured as a CUDA graph takes the same steps as the
-    uncaptured loop: same weights (the step has no order-dependent reductions) and loss
-    history within FP32 rounding of the loss sum."""
+    uncaptured loop: the same weights and loss history up to FP32 rounding (the weight and
+    bias gradients are sums whose order is not fixed: split-K GEMM and column-sum atomics)."""
     import torch
     from chronusq_public_b200.guess_model import PairMLP, NFEAT, MAXF
     rng = np.random.default_rng(5)
@@ -198,5 +199,5 @@ def test_graph_captured_training_matches_uncaptured():
     torch.cuda.synchronize()
     assert a.step == b.step
     for wa, wb in zip(a.W + a.b, b.W + b.b):
-        assert (wa - wb).abs().max().item() <= 1e-6
-    assert np.allclose(ha, hb, rtol=1e-4)
+        assert (wa - wb).abs().max().item() <= 1e-5
+    assert np.allclose(ha, hb, rtol=1e-3)
