@@ -225,7 +225,7 @@ cqg_status cqg_destroy(cqg_ctx *ctx) {
   ctx->d_shmol.release(); ctx->d_mshoff.release(); ctx->d_mnsh.release(); ctx->d_mnbf.release();
   ctx->d_molbk.release(); ctx->d_mxoff.release(); ctx->d_mMoff.release(); ctx->d_active.release();
   ctx->d_prim.release(); ctx->d_boys.release();
-  ctx->d_M.release(); ctx->d_Mmax.release(); ctx->d_flags.release();
+  ctx->d_M.release(); ctx->d_Mmax.release(); ctx->d_Mpair.release(); ctx->d_flags.release();
   ctx->d_cnt.release(); ctx->d_off.release(); ctx->d_range.release(); ctx->d_scan_tmp.release();
   ctx->d_qhead.release();
   ctx->d_qlist.release(); ctx->d_G.release(); ctx->d_X.release(); ctx->d_AX.release(); ctx->d_Gscratch.release();
@@ -513,7 +513,8 @@ cqg_status cqg_set_basis_batch(cqg_ctx *ctx, int nmol, const int *nshell_per_mol
   if (ctx->d_cnt.reserve(2 * task + 1) || ctx->d_off.reserve(2 * task + 1) || ctx->d_range.reserve(4 * CQG_NQC) ||
       ctx->d_qhead.reserve(2 * CQG_NQC + 1) ||
       ctx->d_scan_tmp.reserve(scan_bytes + 16) || ctx->d_M.reserve(2 * (size_t)std::max(ctx->Mtotal, 1LL)) ||
-      ctx->d_Mmax.reserve(1) || ctx->d_flags.reserve(4) || ctx->d_blkacc.reserve(4 * CQG_NQC))
+      ctx->d_Mmax.reserve(1) || ctx->d_flags.reserve(4) || ctx->d_blkacc.reserve(4 * CQG_NQC) ||
+      ctx->d_Mpair.reserve(std::max<size_t>(ctx->pair_sh.size(), 1)))
     return CQG_ERR_OOM;
   return CQG_OK;
 }
@@ -693,17 +694,20 @@ static cqg_status contract_graph(cqg_ctx *ctx, int ngroups, const double *const 
     k_blocknorm<<<g, 128, 0, st>>>(xl, ldx, mols, ctx->d_bf.p, ctx->d_sz.p, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, ctx->d_flags.p, 1e-12);
     const long long nn = ctx->Mtotal;
     k_maxreduce<<<(int)std::min<long long>((nn + 255) / 256, 1184), 256, 0, st>>>(ctx->d_M.p, nn, ctx->d_Mmax.p);
+    const int npairs = (int)ctx->pair_sh.size();
+    k_pairnorm<<<(npairs + 255) / 256, 256, 0, st>>>(ctx->d_pair_sh.p, npairs, mols, ctx->d_shmol.p, ctx->d_M.p,
+                                                     ctx->d_Mpair.p);
   }
   Pairs P = make_pairs(ctx);
   const int nb = (ctx->ntask + 7) / 8;
-  k_quartets<false><<<nb, 256, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
+  k_quartets<false><<<nb, 256, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, ctx->d_Mpair.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
                                          ctx->thresh, cut32, ctx->d_cnt.p, nullptr, nullptr, ctx->d_blkacc.p, 0, 0, 0,
                                          0);
   size_t scan_bytes = ctx->d_scan_tmp.n;
   CUCHK(cub::DeviceScan::ExclusiveSum(ctx->d_scan_tmp.p, scan_bytes, ctx->d_cnt.p, ctx->d_off.p, 2 * ctx->ntask, st));
   k_block_ranges<<<1, 128, 0, st>>>(ctx->bt, ctx->ntask, ctx->d_cnt.p, ctx->d_off.p, ctx->d_range.p,
                                     ctx->graph_capacity, ctx->d_flags.p);
-  k_quartets<true><<<nb, 256, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
+  k_quartets<true><<<nb, 256, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, ctx->d_Mpair.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
                                         ctx->thresh, cut32, nullptr, ctx->d_off.p, ctx->d_qlist.p, nullptr, 0,
                                         2LL * ctx->ntask, 0, ctx->graph_capacity);
   CUCHK(cudaGetLastError());
@@ -721,7 +725,7 @@ static cqg_status contract_graph(cqg_ctx *ctx, int ngroups, const double *const 
     dg.sK[g] = sK[g];
   }
   CUCHK(cudaMemsetAsync(ctx->d_qhead.p, 0, 2 * CQG_NQC * sizeof(unsigned long long), st));
-  int launches = 6;
+  int launches = 7;   // block norms, max, pair norms, list count, scan, ranges, list fill
   if (ctx->fused_tier) {
     cudaError_t e = cqg_launch_fused(ctx, ctx->fused_tier, st, dg);
     ++launches;
@@ -778,15 +782,18 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     long long nn = ctx->Mtotal;
     int nb = (int)std::min<long long>((nn + 255) / 256, 1184);
     k_maxreduce<<<nb, 256, 0, st>>>(ctx->d_M.p, nn, ctx->d_Mmax.p);
+    const int npairs = (int)ctx->pair_sh.size();
+    k_pairnorm<<<(npairs + 255) / 256, 256, 0, st>>>(ctx->d_pair_sh.p, npairs, mols, ctx->d_shmol.p, ctx->d_M.p,
+                                                     ctx->d_Mpair.p);
     CUCHK(cudaGetLastError());
-    ctx->launches += 2;
+    ctx->launches += 3;
   }
   // 2. quartet lists
   Pairs P = make_pairs(ctx);
   {
     int nthr = 256, wpb = nthr / 32;
     int nb = (ctx->ntask + wpb - 1) / wpb;
-    k_quartets<false><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
+    k_quartets<false><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, ctx->d_Mpair.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
                                             ctx->thresh,
                                             cut32, ctx->d_cnt.p, nullptr, nullptr, ctx->d_blkacc.p, 0, 0, 0, 0);
     CUCHK(cudaGetLastError());
@@ -911,7 +918,7 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     {
       int nthr = 256, wpb = nthr / 32;
       int nb = (ctx->ntask + wpb - 1) / wpb;
-      k_quartets<true><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
+      k_quartets<true><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, ctx->d_Mpair.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
                                              ctx->thresh,
                                              cut32, nullptr, ctx->d_off.p, ctx->d_qlist.p, nullptr, vt0, vt1, obase,
                                              (long long)ctx->d_qlist.n);

@@ -224,17 +224,28 @@ __device__ __forceinline__ int coarse_range(const double *__restrict__ Q, int kb
 // density times Q_ab Q_cd (contract.h:112-131).  The four norms that pair a bra shell with
 // a ket shell are read from the transposed copy MT, where M(s1, .) and M(s2, .) are the
 // contiguous columns s1 and s2 (one pair of columns per bra pair, so they stay in L1);
-// m12 = M(s1, s2) is the bra's own, the same for every ket.
-__device__ __forceinline__ double quartet_bound(const double *__restrict__ M, const double *__restrict__ col1,
-                                                const double *__restrict__ col2, double m12, int nsh, int shoff,
-                                                int2 cd, double qab, double qcd) {
+// m12 = M(s1, s2) is the bra's own, the same for every ket, and mcd = M(s3, s4) the ket's
+// own, read from the per-pair copy Mpair (consecutive kets: a coalesced load).
+__device__ __forceinline__ double quartet_bound(const double *__restrict__ col1, const double *__restrict__ col2,
+                                                double m12, double mcd, int shoff, int2 cd, double qab, double qcd) {
   const int s3 = cd.x - shoff, s4 = cd.y - shoff;
   double m = fmax(m12, col1[s4]);
   m = fmax(m, col2[s4]);
-  m = fmax(m, M[s3 + (size_t)s4 * nsh]);
+  m = fmax(m, mcd);
   m = fmax(m, col1[s3]);
   m = fmax(m, col2[s3]);
   return m * qab * qcd;
+}
+
+// Mpair[i] = M(a, b) of shell pair i (its own block norm; molecule-local indices).
+static __global__ void k_pairnorm(const int2 *__restrict__ sh, int npairs, Mols mols, const int *__restrict__ shmol,
+                                  const double *__restrict__ M, double *__restrict__ Mpair) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npairs) return;
+  const int2 ab = sh[i];
+  const int mol = shmol[ab.x];
+  const int nsh = mols.nsh[mol], shoff = mols.shoff[mol];
+  Mpair[i] = M[mols.Moff[mol] + (ab.x - shoff) + (size_t)(ab.y - shoff) * nsh];
 }
 
 // Count (FILL=false) or write (FILL=true) the passing quartets of each task.  One warp
@@ -243,7 +254,8 @@ __device__ __forceinline__ double quartet_bound(const double *__restrict__ M, co
 // (counts cnt[ntask + task], offsets off[ntask + task]); the rest to the FP64 list.
 template <bool FILL>
 __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pairs P, const double *__restrict__ M,
-                                                  const double *__restrict__ MT, Mols mols, const int *__restrict__ shmol,
+                                                  const double *__restrict__ MT, const double *__restrict__ Mpair,
+                                                  Mols mols, const int *__restrict__ shmol,
                                                   const double *__restrict__ Mmax, double thresh,
                                                   double cut32, long long *__restrict__ cnt,
                                                   const long long *__restrict__ off, uint2 *__restrict__ qlist,
@@ -282,7 +294,7 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
         int ket = k0 + lane;
         bool pass = false, lo = false;
         if (ket < kend) {
-          const double bnd = quartet_bound(Mm, col1, col2, m12, nsh, shoff, P.sh[ket], qb, P.Q[ket]);
+          const double bnd = quartet_bound(col1, col2, m12, Mpair[ket], shoff, P.sh[ket], qb, P.Q[ket]);
           pass = bnd >= thresh;
           lo = pass && bnd < cut32;
         }
@@ -1198,7 +1210,7 @@ struct cqg_ctx {
   long long prim_pairs_total = 0;
   std::vector<int> pair_np_host;
   // per-call scratch
-  DevBuf<double> d_M, d_Mmax;
+  DevBuf<double> d_M, d_Mmax, d_Mpair;
   DevBuf<int> d_flags;
   DevBuf<long long> d_cnt, d_off, d_range;
   DevBuf<unsigned char> d_scan_tmp;

@@ -13,13 +13,14 @@ nearest the pair midpoint), so what it predicts is a local-frame block.  The blo
 carried to the molecular frame by the exact rotation matrices of the basis functions
 (1 for s, the frame matrix for Cartesian p, the real-solid-harmonic rotation for pure d
 and f), which makes the assembled density equivariant under rotations and translations by
-construction.  Pairs are ordered heavier element first; one network whose MAXF x MAXF
-output is masked per pair type serves every pair type of the basis.
+construction.  Pairs are ordered heavier element first; one network whose maxf x maxf
+output (maxf: the largest function count of one atom in the basis, head_size) is masked
+per pair type serves every pair type of the basis.
 
-Training and inference run through the library's BF16 kernels (csrc/mlp.cu: GEMM with
-fused bias and SiLU, SiLU backward, bias reduction, masked MSE, Adam); torch only holds
-device memory.  The SCF uses a prediction as a READ guess (one Fock build from it,
-diagonalised), so the guess can change the iteration count but not the converged answer.
+Training and inference run through the library's kernels (csrc/mlp.cu: BF16 tensor-core
+GEMM with fused bias and SiLU, SiLU backward, bias reduction, masked MSE, Adam); torch only
+holds device memory.  The SCF starts its iterations from the natural-orbital projection of
+a prediction, so the guess can change the iteration count but not the converged answer.
 """
 from __future__ import annotations
 
@@ -37,7 +38,7 @@ from .basis import BasisSet, cart_list, solid_harmonic_matrix
 ELEMS = (1, 8)                 # element vocabulary (H, O)
 KNEIGH = 8                     # environment atoms per pair
 NFEAT = 2 * len(ELEMS) + 4 + KNEIGH * (4 + len(ELEMS)) + 1
-MAXF = 14                      # largest per-atom function count handled (O in 6-31G(d) and cc-pVDZ)
+MAXF = 14                      # default head: largest per-atom function count (O in 6-31G(d) and cc-pVDZ)
 
 
 # ---------------------------------------------------------------- rotations ---
@@ -103,7 +104,8 @@ class AtomLayout:
     """Per atom of a molecule: element, first basis function and function count; per
     element its (l, pure) shell list (the same for every atom of an element in a basis)."""
 
-    def __init__(self, Z: Sequence[int], bs: BasisSet):
+    def __init__(self, Z: Sequence[int], bs: BasisSet, maxf: int = MAXF):
+        self.maxf = int(maxf)
         self.Z = np.asarray(Z, dtype=np.int64)
         n = len(self.Z)
         self.off = np.full(n, -1, dtype=np.int64)
@@ -122,8 +124,8 @@ class AtomLayout:
             if z in self.shells and self.shells[z] != per_atom[a]:
                 raise ValueError("atoms of one element carry different shells")
             self.shells[z] = per_atom[a]
-        if int(self.nf.max()) > MAXF:
-            raise ValueError("an atom has %d functions; the model handles at most %d" % (self.nf.max(), MAXF))
+        if int(self.nf.max()) > self.maxf:
+            raise ValueError("an atom has %d functions; the model handles at most %d" % (self.nf.max(), self.maxf))
 
 
 # ---------------------------------------------------------------- pairs, frames, features ---
@@ -210,10 +212,11 @@ def _block_index(layout, pairs, idx, na, nb):
 
 
 def local_blocks(layout: AtomLayout, pairs, F, P: np.ndarray):
-    """Targets Wa^T P_ab Wb in the pair frames and their masks, padded to MAXF x MAXF."""
+    """Targets Wa^T P_ab Wb in the pair frames and their masks, padded to maxf x maxf."""
     npair = len(pairs)
-    T = np.zeros((npair, MAXF, MAXF))
-    M = np.zeros((npair, MAXF, MAXF), dtype=np.float32)
+    mf = layout.maxf
+    T = np.zeros((npair, mf, mf))
+    M = np.zeros((npair, mf, mf), dtype=np.float32)
     for (za, zb), idx in pair_type_groups(layout, pairs).items():
         Wa, Wb = atom_rotations(layout.shells[za], F[idx]), atom_rotations(layout.shells[zb], F[idx])
         na, nb = Wa.shape[1], Wb.shape[1]
@@ -224,9 +227,9 @@ def local_blocks(layout: AtomLayout, pairs, F, P: np.ndarray):
 
 
 def assemble_density(layout: AtomLayout, pairs, F, blocks: np.ndarray, nbf: int) -> np.ndarray:
-    """Molecular-frame density from local-frame blocks (P, MAXF*MAXF); pairs not listed
+    """Molecular-frame density from local-frame blocks (P, maxf*maxf); pairs not listed
     (farther apart than the cut-off) stay zero."""
-    B = np.asarray(blocks).reshape(-1, MAXF, MAXF)
+    B = np.asarray(blocks).reshape(-1, layout.maxf, layout.maxf)
     D = np.zeros((nbf, nbf))
     for (za, zb), idx in pair_type_groups(layout, pairs).items():
         Wa, Wb = atom_rotations(layout.shells[za], F[idx]), atom_rotations(layout.shells[zb], F[idx])
@@ -241,12 +244,12 @@ def assemble_density(layout: AtomLayout, pairs, F, blocks: np.ndarray, nbf: int)
     return D
 
 
-def molecule_samples(mol, bs: BasisSet, rcut: float, P: np.ndarray = None):
+def molecule_samples(mol, bs: BasisSet, rcut: float, P: np.ndarray = None, maxf: int = MAXF):
     """(layout, pairs, frames, features) of one molecule, plus (targets, masks) when the
-    density P is given."""
+    density P is given; blocks are padded to the head size `maxf`."""
     Z = np.asarray(mol.atoms, dtype=np.int64)
     R = np.asarray(mol.coords, dtype=np.float64).reshape(-1, 3)
-    layout = AtomLayout(Z, bs)
+    layout = AtomLayout(Z, bs, maxf)
     pairs = canonical_pairs(Z, R, rcut)
     F, X = frames_and_features(Z, R, pairs)
     if P is None:
@@ -257,17 +260,21 @@ def molecule_samples(mol, bs: BasisSet, rcut: float, P: np.ndarray = None):
 
 # ---------------------------------------------------------------- the network ---
 class PairMLP:
-    """NFEAT -> width (x `layers` hidden layers, SiLU) -> MAXF*MAXF; BF16 operands and
-    activations, FP32 accumulation, FP32 master weights updated by Adam."""
+    """NFEAT -> width (x `layers` hidden layers, SiLU) -> maxf*maxf; BF16 operands and
+    activations, FP32 accumulation, FP32 master weights updated by Adam.  `maxf` is the
+    head's per-atom block size: the largest function count of one atom in the basis the
+    model predicts in (14 for O in 6-31G(d) and cc-pVDZ, 30 in cc-pVTZ; head_size)."""
 
-    def __init__(self, width: int = 256, layers: int = 4, seed: int = 0, device: int = 0, rcut: float = 8.0):
+    def __init__(self, width: int = 256, layers: int = 4, seed: int = 0, device: int = 0, rcut: float = 8.0,
+                 maxf: int = MAXF):
         import torch
         self.torch = torch
         self.L = _lib.lib()
         self.dev = torch.device("cuda", device)
         self.rcut = float(rcut)
+        self.maxf = int(maxf)
         rng = np.random.default_rng(seed)
-        self.dims = [NFEAT] + [width] * layers + [MAXF * MAXF]
+        self.dims = [NFEAT] + [width] * layers + [self.maxf * self.maxf]
         W, b = [], []
         for i in range(len(self.dims) - 1):
             w = rng.normal(0.0, 1.0 / math.sqrt(self.dims[i]), size=(self.dims[i + 1], self.dims[i]))
@@ -278,7 +285,7 @@ class PairMLP:
         self.set_weights(W, b)
         self.xmean = np.zeros(NFEAT)
         self.xstd = np.ones(NFEAT)
-        self.ymean = np.zeros(MAXF * MAXF)
+        self.ymean = np.zeros(self.maxf * self.maxf)
         self.ystd = 1.0
 
     def set_weights(self, W, b):
@@ -301,7 +308,7 @@ class PairMLP:
 
     # ------------------------------------------------------------------ passes ---
     def forward(self, Xbf, keep: bool = False):
-        """Xbf (M, NFEAT) BF16 -> FP32 output (M, MAXF*MAXF).  keep: also return, per
+        """Xbf (M, NFEAT) BF16 -> FP32 output (M, maxf*maxf).  keep: also return, per
         layer, its BF16 input and FP32 pre-activation for the backward pass."""
         t = self.torch
         M = Xbf.shape[0]
@@ -321,7 +328,7 @@ class PairMLP:
         return out, cache
 
     def backward(self, dout, cache):
-        """dout (M, MAXF*MAXF) FP32 = dLoss/dOutput -> FP32 weight and bias gradients."""
+        """dout (M, maxf*maxf) FP32 = dLoss/dOutput -> FP32 weight and bias gradients."""
         t = self.torch
         nl = len(self.W)
         gW, gb = [None] * nl, [None] * nl
@@ -469,7 +476,7 @@ class PairMLP:
 
     def predict(self, X: np.ndarray) -> np.ndarray:
         if len(X) == 0:
-            return np.zeros((0, MAXF * MAXF))
+            return np.zeros((0, self.maxf * self.maxf))
         out, _ = self.forward(self.normalise_inputs(X))
         return out.double().cpu().numpy() * self.ystd + self.ymean
 
@@ -489,9 +496,10 @@ class PairMLP:
     def load(cls, path: str, device: int = 0) -> "PairMLP":
         d = np.load(path)
         dims = [int(x) for x in d["dims"]]
-        if dims[0] != NFEAT or dims[-1] != MAXF * MAXF or int(d["kneigh"]) != KNEIGH:
+        maxf = int(round(math.sqrt(dims[-1])))
+        if dims[0] != NFEAT or maxf * maxf != dims[-1] or int(d["kneigh"]) != KNEIGH:
             raise ValueError("weights were made for another feature layout")
-        m = cls(width=dims[1], layers=len(dims) - 2, device=device, rcut=float(d["rcut"]))
+        m = cls(width=dims[1], layers=len(dims) - 2, device=device, rcut=float(d["rcut"]), maxf=maxf)
         nl = len(dims) - 1
         m.set_weights([d["W%d" % i] for i in range(nl)], [d["b%d" % i] for i in range(nl)])
         m.xmean, m.xstd = d["xmean"], d["xstd"]
@@ -508,10 +516,16 @@ def default_weights(basis: str):
     return path if os.path.exists(path) else None
 
 
+def head_size(basis: str) -> int:
+    """Head block size a network needs for `basis`: the largest function count of one atom
+    of the model's elements in that basis."""
+    return max(BasisSet(basis, [z], np.zeros((1, 3))).nbasis for z in ELEMS)
+
+
 def predict_densities(model: PairMLP, mols, bss) -> List[np.ndarray]:
     """Molecular densities assembled from the network's local-frame pair blocks; the
     pairs of all molecules go through one forward pass."""
-    samples = [molecule_samples(m, bs, model.rcut) for m, bs in zip(mols, bss)]
+    samples = [molecule_samples(m, bs, model.rcut, maxf=model.maxf) for m, bs in zip(mols, bss)]
     Y = model.predict(np.concatenate([s[3] for s in samples]))
     out, o = [], 0
     for (layout, pairs, F, X), bs in zip(samples, bss):

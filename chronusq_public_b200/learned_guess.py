@@ -24,7 +24,7 @@ from typing import Dict, List, Sequence
 import numpy as np
 
 from .basis import BasisSet
-from .guess_model import PairMLP, molecule_samples
+from .guess_model import PairMLP, head_size, molecule_samples
 from .molecule import Molecule, single_water, water_cluster
 
 
@@ -56,10 +56,10 @@ def converged_densities(mols: Sequence[Molecule], basis: str, chunk: int = 512, 
     return P_out, np.array(E_out), np.array(it_out), secs
 
 
-def training_arrays(mols: Sequence[Molecule], basis: str, densities, rcut: float):
+def training_arrays(mols: Sequence[Molecule], basis: str, densities, rcut: float, maxf: int):
     X, T, M = [], [], []
     for mol, P in zip(mols, densities):
-        _, _, _, x, t, m = molecule_samples(mol, BasisSet(basis, mol.atoms, mol.coords), rcut, P)
+        _, _, _, x, t, m = molecule_samples(mol, BasisSet(basis, mol.atoms, mol.coords), rcut, P, maxf)
         X.append(x)
         T.append(t)
         M.append(m)
@@ -75,9 +75,10 @@ def train(basis: str = "6-31g*", ntrain: int = 4000, nmin: int = 2, nmax: int = 
     mols = cluster_set(ntrain, nmin, nmax, seed)
     P, E, its, scf_s = converged_densities(mols, basis)
     t1 = time.perf_counter()
-    X, T, M = training_arrays(mols, basis, P, rcut)
+    maxf = head_size(basis)
+    X, T, M = training_arrays(mols, basis, P, rcut, maxf)
     t2 = time.perf_counter()
-    model = PairMLP(width=width, layers=layers, seed=seed, rcut=rcut)
+    model = PairMLP(width=width, layers=layers, seed=seed, rcut=rcut, maxf=maxf)
     hist = model.fit(X, T, M, epochs=epochs, lr=lr, log=(lambda e, l: log("epoch %d loss %.3e" % (e, l))) if log else None)
     model.torch.cuda.synchronize()
     t3 = time.perf_counter()
