@@ -56,7 +56,10 @@ def converged_densities(mols: Sequence[Molecule], basis: str, chunk: int = 512, 
     return P_out, np.array(E_out), np.array(it_out), secs
 
 
-def training_arrays(mols: Sequence[Molecule], basis: str, densities, rcut: float, maxf: int):
+def training_arrays(mols: Sequence[Molecule], basis: str, densities, rcut: float, maxf: int = None):
+    """Features, local-frame targets and masks of every pair of `mols`, blocks padded to the
+    head size `maxf` (default: the basis's, head_size)."""
+    maxf = head_size(basis) if maxf is None else maxf
     X, T, M = [], [], []
     for mol, P in zip(mols, densities):
         _, _, _, x, t, m = molecule_samples(mol, BasisSet(basis, mol.atoms, mol.coords), rcut, P, maxf)
