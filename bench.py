@@ -274,6 +274,9 @@ def schedule_summary(ints, st):
     tier, tuned = ints.fusion()
     out = {"fusion": {"tier": tier, "fused_kernel_ms": round(st.get("ms_fused", 0.0), 4),
                       "tuned_ms_tier0_1_2": [round(x, 4) for x in tuned]}}
+    from chronusq_public_b200 import _lib
+    lists = _lib.schedule_lists()
+    sib = set(st.get("sibling_classes", []))
     for k, (name, nq) in enumerate(st["class_quartets"].items()):
         if nq <= 0:
             continue
@@ -281,6 +284,9 @@ def schedule_summary(ints, st):
         form = "fused" if fused else ("warp" if sch["warp_form"][k] else "thread")
         out[name] = {"form": form, "cta_per_sm": sch["cta_per_sm"][k], "warps_per_cta": sch["warps_per_cta"][k],
                      "quartets_per_warp": sch["quartets_per_warp"][k], "ms": round(st["class_ms"][name], 4)}
+        if name in sib:   # the class's sibling-group list (its time is in the class's ms)
+            b = lists.index(name + " siblings")
+            out[name]["siblings"] = {"cta_per_sm": sch["cta_per_sm"][b], "quartets_per_warp": sch["quartets_per_warp"][b]}
     return out
 
 
@@ -292,6 +298,7 @@ def config_of(args, w, bs):
             "geometry": "seeded water cluster at 1.0 g/cm^3 (Poisson-disk O centres, min O-O 2.6 A)",
             "l2": "flushed between steps (256 MiB write)",
             "precision": "fp64", "parallelism": "replicas" if args.gpus > 1 else "single",
+            "sibling_groups": getattr(args, "siblings", "off"),
             "launch_shapes": ("from %s" % os.path.basename(args.schedule_in) if getattr(args, "schedule_in", None)
                               else "default" if args.no_autotune else "autotuned in the first warm-up build")}
 
@@ -437,6 +444,10 @@ def main():
     ap.add_argument("--no-sweep", action="store_true", help="skip the FP32 cutoff sweep 1e-10..1e-6")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes instead of autotuned ones")
+    ap.add_argument("--siblings", default="off", choices=["on", "off"],
+                    help="sibling-group lists for the segmented shells of one general contraction")
+    ap.add_argument("--sibling-min", default="",
+                    help="per sibling class, the member quartets a sibling entry holds at least, e.g. '(ss|ss)=8,(ps|ss)=4'")
     ap.add_argument("--fusion", default="auto", choices=["auto", "0", "1", "2"],
                     help="class-fusion tier of the benchmarked builds (auto: the autotuner's choice)")
     ap.add_argument("--schedule-out", default=None, help="write the autotuned per-list schedule to this JSON file")
@@ -473,6 +484,10 @@ def main():
     w, mol, bs, D = build_workload(args.workload, args.density)
     n = bs.nbasis
     ints = AOIntegrals(bs, device=local, thresholdSchwartz=w["thresh"])
+    ints.setSiblings(args.siblings == "on")
+    for item in filter(None, args.sibling_min.split(",")):
+        cls, m = item.split("=")
+        ints.setSiblingMin(cls.strip(), int(m))
     Dd = torch.from_numpy(D).cuda()
     PT = torch.zeros_like(Dd)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -494,7 +509,7 @@ def main():
             json.dump(dict(ints.schedule(), fusion_tier=ints.fusion()[0]), f)
     ints.setTiming(True)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    step_ms, eri_ms, quartets, mflops, launches, class_ms = [], [], [], [], 0, {}
+    step_ms, eri_ms, quartets, mflops, launches, class_ms, screen_ms = [], [], [], [], 0, {}, []
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
@@ -509,6 +524,7 @@ def main():
             quartets.append(st["quartets"])
             mflops.append(st["model_flops"])
             eri_ms.append(st["ms_eri"])
+            screen_ms.append(st["ms_screen"])
             launches += st["launches"]
             for c, v in st["class_ms"].items():
                 class_ms[c] = class_ms.get(c, 0.0) + v / args.steps
@@ -562,6 +578,8 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": config_of(args, w, bs),
             "quartets_per_step": quartets[0], "fock_builds_per_s": 1e3 * args.steps / tot_ms,
+            "screen_ms_per_step": sum(screen_ms) / len(screen_ms),
+            "list_entries_per_step": st_last["list_entries"],
             "e2e": {"value": e2e_val, "unit": "quartets/s", "h2d_bytes_per_step": 2 * n * n * 8,
                     "d2h_bytes_per_step": n * n * 8, "max_abs_diff_vs_device_path": err},
             "roofline": {"bound": "fp64", "kernel": "k_eri_jk (all quartet classes, ERI + J/K digest)",

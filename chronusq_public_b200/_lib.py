@@ -34,7 +34,8 @@ EXPORTED = [
     "cqg_set_graph_mode", "cqg_graph_status", "cqg_autotune_next", "cqg_get_launch_shapes", "cqg_set_active",
     "cqg_mlp_gemm_bf16", "cqg_mlp_silu_bwd", "cqg_mlp_to_bf16", "cqg_mlp_colsum", "cqg_mlp_mse", "cqg_mlp_adam",
     "cqg_one_e_noalloc", "cqg_dipole", "cqg_get_schedule", "cqg_set_schedule",
-    "cqg_set_fusion", "cqg_get_fusion", "cqg_mlp_adam_dev",
+    "cqg_set_fusion", "cqg_get_fusion", "cqg_mlp_adam_dev", "cqg_set_siblings", "cqg_get_siblings",
+    "cqg_schedule_lists", "cqg_list_class", "cqg_set_sibling_min",
 ]
 
 
@@ -54,6 +55,8 @@ class CqgStats(ctypes.Structure):
         ("class_ms", ctypes.c_double * 55),
         ("ms_fused", ctypes.c_double),
         ("fused_tier", ctypes.c_int),
+        ("list_entries", ctypes.c_longlong),
+        ("sibling_classes", ctypes.c_longlong),
     ]
 
 
@@ -97,6 +100,11 @@ def load(path: str = LIB_PATH):
     L.cqg_set_schedule.argtypes = [vp, i, i, i, i]
     L.cqg_set_fusion.argtypes = [vp, ctypes.c_int]
     L.cqg_get_fusion.argtypes = [vp, i, d]
+    L.cqg_set_siblings.argtypes = [vp, ctypes.c_int]
+    L.cqg_get_siblings.argtypes = [vp, i]
+    L.cqg_schedule_lists.argtypes = []
+    L.cqg_list_class.argtypes = [ctypes.c_int]
+    L.cqg_set_sibling_min.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     L.cqg_set_active.argtypes = [vp, ctypes.c_char_p]
     ll, f, fp = ctypes.c_longlong, ctypes.c_float, ctypes.POINTER(ctypes.c_float)
     L.cqg_mlp_gemm_bf16.argtypes = [vp, ll, ll, vp, ll, ll, vp, ll, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp,
@@ -120,7 +128,9 @@ def load(path: str = LIB_PATH):
                  "cqg_twoe_contract_direct_batch", "cqg_one_e_batch", "cqg_set_graph_mode",
                  "cqg_graph_status", "cqg_autotune_next", "cqg_get_launch_shapes", "cqg_set_active",
                  "cqg_mlp_gemm_bf16", "cqg_mlp_silu_bwd", "cqg_mlp_to_bf16", "cqg_mlp_colsum", "cqg_mlp_mse",
-                 "cqg_mlp_adam", "cqg_one_e_noalloc", "cqg_dipole", "cqg_get_schedule", "cqg_set_schedule", "cqg_set_fusion", "cqg_get_fusion", "cqg_mlp_adam_dev"]:
+                 "cqg_mlp_adam", "cqg_one_e_noalloc", "cqg_dipole", "cqg_get_schedule", "cqg_set_schedule", "cqg_set_fusion", "cqg_get_fusion", "cqg_mlp_adam_dev",
+                 "cqg_set_siblings", "cqg_get_siblings", "cqg_schedule_lists", "cqg_list_class",
+                 "cqg_set_sibling_min"]:
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -136,6 +146,20 @@ def check(status: int, ctx=None):
         if ctx:
             msg = (lib().cqg_last_error(ctx) or b"").decode()
         raise CqgError(status, msg)
+
+
+def schedule_lists():
+    """Names of the schedule's work lists, in cqg_get_schedule order: the FP64 then the FP32
+    pair-entry lists of the quartet classes, then their FP64 and FP32 sibling-entry lists
+    ("(ss|ss) siblings")."""
+    L = lib()
+    names = class_names()
+    n = int(L.cqg_schedule_lists())
+    out = []
+    for b in range(n):
+        k = int(L.cqg_list_class(b))
+        out.append(names[k] + (" siblings" if b >= n // 2 else ""))
+    return out
 
 
 def class_names():

@@ -129,10 +129,12 @@ class AOIntegrals:
         return sch["cta_per_sm"], sch["warps_per_cta"]
 
     def schedule(self):
-        """Per class work list (FP64 lists then FP32 lists, 110 entries each): CTAs per SM,
-        warps per CTA and quartets claimed per warp (0 = default), and the kernel form
-        (1 = warp-cooperative, 0 = one quartet per thread)."""
-        out = [(ctypes.c_int * 110)() for _ in range(4)]
+        """Per work list (lists named by ``_lib.schedule_lists()``: FP64 lists then FP32
+        lists, each the quartet classes then the sibling-group lists): CTAs per SM, warps per
+        CTA and quartets claimed per warp (0 = default), and the kernel form (1 =
+        warp-cooperative, 0 = one quartet per thread)."""
+        n = int(self._L.cqg_schedule_lists())
+        out = [(ctypes.c_int * n)() for _ in range(4)]
         _lib.check(self._L.cqg_get_schedule(self._ctx, *out), self._ctx)
         return {k: list(v) for k, v in zip(("cta_per_sm", "warps_per_cta", "quartets_per_warp", "warp_form"), out)}
 
@@ -148,16 +150,37 @@ class AOIntegrals:
         _lib.check(self._L.cqg_get_fusion(self._ctx, ctypes.byref(t), ms), self._ctx)
         return int(t.value), list(ms)
 
+    def setSiblings(self, on: bool):
+        """Sibling groups on / off (default): (ss|ss), (ps|ss), (ps|ps), (pp|ss) and (ds|ss)
+        get lists of entries of sibling shell pairs (same centres, angular momenta and
+        exponents), evaluated from one pass over their shared primitive pairs.  The quartets,
+        their count and the result are those of the pair-level lists."""
+        _lib.check(self._L.cqg_set_siblings(self._ctx, 1 if on else 0), self._ctx)
+
+    def setSiblingMin(self, cls: str, min_members: int):
+        """Sibling class `cls` ("(ss|ss)"): a pair of sibling groups becomes one sibling entry
+        when it holds at least `min_members` member quartets; smaller ones run as pair
+        quartets."""
+        k = _lib.class_names().index(cls)
+        _lib.check(self._L.cqg_set_sibling_min(self._ctx, k, int(min_members)), self._ctx)
+
+    def siblings(self) -> bool:
+        v = ctypes.c_int()
+        _lib.check(self._L.cqg_get_siblings(self._ctx, ctypes.byref(v)), self._ctx)
+        return bool(v.value)
+
     def setSchedule(self, cta_per_sm=None, warps_per_cta=None, quartets_per_warp=None, warp_form=None):
-        """Set the per-list schedule (sequences of 110 ints as :meth:`schedule` returns them,
-        or one int for every list; None leaves that part unchanged)."""
+        """Set the per-list schedule (sequences as :meth:`schedule` returns them, or one int
+        for every list; None leaves that part unchanged)."""
+        n = int(self._L.cqg_schedule_lists())
+
         def arr(v):
             if v is None:
                 return None
-            v = [int(v)] * 110 if isinstance(v, (int, np.integer)) else [int(x) for x in v]
-            if len(v) != 110:
-                raise ValueError("a schedule has 110 entries (55 FP64 lists, 55 FP32 lists)")
-            return (ctypes.c_int * 110)(*v)
+            v = [int(v)] * n if isinstance(v, (int, np.integer)) else [int(x) for x in v]
+            if len(v) != n:
+                raise ValueError("a schedule has %d entries (FP64 lists, then FP32 lists)" % n)
+            return (ctypes.c_int * n)(*v)
         _lib.check(self._L.cqg_set_schedule(self._ctx, arr(cta_per_sm), arr(warps_per_cta), arr(quartets_per_warp),
                                             arr(warp_form)), self._ctx)
 
@@ -182,6 +205,8 @@ class AOIntegrals:
             "class_quartets": {names[k]: int(s.class_quartets[k]) for k in range(len(names))},
             "class_ms": {names[k]: float(s.class_ms[k]) for k in range(len(names))},
             "ms_fused": float(s.ms_fused), "fused_tier": int(s.fused_tier),
+            "list_entries": int(s.list_entries),
+            "sibling_classes": [names[k] for k in range(len(names)) if (int(s.sibling_classes) >> k) & 1],
         }
 
     # ------------------------------------------------------------------ contraction ---

@@ -119,8 +119,9 @@ class BatchAOIntegrals:
         _lib.check(self._L.cqg_autotune_next(self._ctx), self._ctx)
 
     def launch_shapes(self):
-        cta = np.zeros(110, dtype=np.int32)
-        wpb = np.zeros(110, dtype=np.int32)
+        n = int(self._L.cqg_schedule_lists())
+        cta = np.zeros(n, dtype=np.int32)
+        wpb = np.zeros(n, dtype=np.int32)
         i = ctypes.POINTER(ctypes.c_int)
         _lib.check(self._L.cqg_get_launch_shapes(self._ctx, cta.ctypes.data_as(i), wpb.ctypes.data_as(i)), self._ctx)
         return cta, wpb

@@ -37,6 +37,7 @@ def _nvcc():
 
 def _sources():
     return (glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cuh")) +
+            glob.glob(os.path.join(CSRC, "*.h")) +
             glob.glob(os.path.join(CSRC, "*.py")) + glob.glob(os.path.join(INCLUDE, "*.h")))
 
 

@@ -14,6 +14,7 @@
 //                      the scales are folded into the digest).
 #include "engine_impl.cuh"
 #include "one_e.cuh"
+#include "siblings.h"
 
 static const char *kLetters = "spdfg";
 static char g_class_names[55][16];
@@ -80,10 +81,10 @@ static void pair_prims(const cqg_ctx *ctx, int a, int b, double prim_thresh, std
 
 // primitive-count bucket of a shell pair: warps of the ERI kernels see kets of one bucket
 static inline int prim_bucket(int np) {
-  static const int upper[CQG_NBUCKET - 1] = {1, 2, 3, 4, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64};
-  for (int b = 0; b < CQG_NBUCKET - 1; ++b)
+  static const int upper[CQG_NPBUCKET - 1] = {1, 2, 3, 4, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64};
+  for (int b = 0; b < CQG_NPBUCKET - 1; ++b)
     if (np <= upper[b]) return b;
-  return CQG_NBUCKET - 1;
+  return CQG_NPBUCKET - 1;
 }
 
 // build primitive-pair data for the current pair ordering and upload all pair arrays
@@ -116,9 +117,186 @@ static cqg_status upload_pairs(cqg_ctx *ctx, double prim_thresh) {
   return CQG_OK;
 }
 
+// Unit-coefficient primitive pairs of a sibling group and its members' coefficient
+// products.  members[0] leads the group; the primitive pair (ia, ib) couples primitive ia of
+// the leader's first shell with primitive ib of its second (the members share the
+// exponents).  A primitive pair is kept when any member's bound |c_a c_b K| of pair_prims
+// reaches prim_thresh (the union of the members' screened primitive pairs).  w gets `rows`
+// rows, one value per kept primitive pair: row k = member k's products c_a(ia) c_b(ib), zero
+// for the rows past the last member.
+static void group_prims(const cqg_ctx *ctx, const int *members, int m, int rows, double prim_thresh,
+                        const std::vector<int> &fam, std::vector<PrimPair> &out, std::vector<double> &w) {
+  const double pi = 3.14159265358979323846;
+  const double s2pi52 = std::sqrt(2.0 * std::pow(pi, 2.5));
+  const int a = ctx->pair_sh[members[0]].x, b = ctx->pair_sh[members[0]].y;
+  const double *A = &ctx->hcent[3 * a], *B = &ctx->hcent[3 * b];
+  double AB2 = 0;
+  for (int x = 0; x < 3; ++x) AB2 += (A[x] - B[x]) * (A[x] - B[x]);
+  const double ABn = std::sqrt(AB2);
+  // coefficient arrays of each member, in the leader's shell order
+  std::vector<const double *> ca(m), cb(m);
+  for (int k = 0; k < m; ++k) {
+    const int x = ctx->pair_sh[members[k]].x, y = ctx->pair_sh[members[k]].y;
+    const bool same = cqg_sib::same_orientation(x, a, fam);
+    ca[k] = &ctx->hcoef[ctx->hpoff[same ? x : y]];
+    cb[k] = &ctx->hcoef[ctx->hpoff[same ? y : x]];
+  }
+  std::vector<std::vector<double>> wk(rows);
+  for (int ia = 0; ia < ctx->hnprim[a]; ++ia)
+    for (int ib = 0; ib < ctx->hnprim[b]; ++ib) {
+      const double al = ctx->halpha[ctx->hpoff[a] + ia], be = ctx->halpha[ctx->hpoff[b] + ib];
+      const double p = al + be;
+      const double K = std::exp(-al * be / p * AB2);
+      bool keep = prim_thresh <= 0;
+      if (!keep) {
+        const double f = s2pi52 / (p * std::pow(2.0 * p, 0.25)) * std::pow(1.0 + ABn, ctx->hL[a] + ctx->hL[b]);
+        for (int k = 0; k < m && !keep; ++k) keep = std::fabs(ca[k][ia] * cb[k][ib] * K) * f >= prim_thresh;
+      }
+      if (!keep) continue;
+      PrimPair pp;
+      pp.p = p;
+      pp.ip = 1.0 / p;
+      pp.Kp = s2pi52 * K / p;
+      pp.Px = (al * A[0] + be * B[0]) / p;
+      pp.Py = (al * A[1] + be * B[1]) / p;
+      pp.Pz = (al * A[2] + be * B[2]) / p;
+      out.push_back(pp);
+      for (int k = 0; k < rows; ++k) wk[k].push_back(k < m ? ca[k][ia] * cb[k][ib] : 0.0);
+    }
+  for (int k = 0; k < rows; ++k) w.insert(w.end(), wk[k].begin(), wk[k].end());
+}
+
+// Quartet class k has the sibling form (its lists hold group entries when siblings are on).
+static bool class_grouped(int k) {
+  static bool table[CQG_NQC];
+  static bool init = false;
+  if (!init) {
+    for (int q = 0; q < CQG_NQC; ++q) table[q] = false;
+#define CQG_GC_MARK(A, B, C, D, MB, MK) \
+  table[pair_class_of(A, B) * (pair_class_of(A, B) + 1) / 2 + pair_class_of(C, D)] = true;
+    CQG_GC_EACH(CQG_GC_MARK)
+#undef CQG_GC_MARK
+    init = true;
+  }
+  return k >= 0 && k < CQG_NQC && table[k];
+}
+
+// Default smallest member count of a sibling entry: half of the sibling form's MB x MK
+// quartets (a pair of groups that fills less of the form runs as separate pair quartets).
+static int default_sibling_min(int k) {
+#define CQG_GC_MIN(A, B, C, D, MB, MK) \
+  if (k == pair_class_of(A, B) * (pair_class_of(A, B) + 1) / 2 + pair_class_of(C, D)) return (MB * MK + 1) / 2;
+  CQG_GC_EACH(CQG_GC_MIN)
+#undef CQG_GC_MIN
+  return 0;
+}
+
+// Pair classes that are the bra or ket of a sibling class (their pairs get group data).
+static bool pair_class_in_groups(int c) {
+  for (int k = 0; k < CQG_NQC; ++k) {
+    if (!class_grouped(k)) continue;
+    int i, j;
+    qclass_split(k, i, j);
+    if (i == c || j == c) return true;
+  }
+  return false;
+}
+
+// Group data of the current pair order (leaders: unit primitive pairs and member weights)
+// and the group index arrays, to the device.
+static cqg_status upload_groups(cqg_ctx *ctx, const std::vector<int> &fam, double prim_thresh) {
+  const int np = (int)ctx->pair_sh.size();
+  std::vector<int> gpoff(np, 0), gnp(np, 0), gwoff(np, 0);
+  std::vector<PrimPair> prim;
+  std::vector<double> w;
+  std::vector<int> members;
+  for (int c = 0; c < CQG_NPC; ++c) {
+    if (!pair_class_in_groups(c)) continue;
+    const int rows = sibling_cap(kPairClass[c][0], kPairClass[c][1]);
+    for (int i = ctx->pc_beg[c]; i < ctx->pc_beg[c + 1]; ++i) {
+      const int m = ctx->pair_gsz[i];
+      if (m == 0) continue;   // not a leader
+      members.resize(m);
+      for (int k = 0; k < m; ++k) members[k] = i + k;
+      gpoff[i] = (int)prim.size();
+      gwoff[i] = (int)w.size();
+      group_prims(ctx, members.data(), m, rows, prim_thresh, fam, prim, w);
+      gnp[i] = (int)prim.size() - gpoff[i];
+    }
+  }
+  const size_t ng = ctx->glead.size();
+  if (ctx->d_pair_Qc.reserve(np) || ctx->d_gsz.reserve(np) || ctx->d_gpoff.reserve(np) || ctx->d_gnp.reserve(np) ||
+      ctx->d_gwoff.reserve(np) || ctx->d_gprim.reserve(std::max<size_t>(prim.size(), 1)) ||
+      ctx->d_gw.reserve(std::max<size_t>(w.size(), 1)) || ctx->d_glead.reserve(std::max<size_t>(ng, 1)) ||
+      ctx->d_gQ.reserve(std::max<size_t>(ng, 1))) {
+    ctx->err = "device allocation for sibling-group data failed";
+    return CQG_ERR_OOM;
+  }
+  CUCHK(cudaMemcpy(ctx->d_pair_Qc.p, ctx->pair_Qc.data(), np * sizeof(double), cudaMemcpyHostToDevice));
+  CUCHK(cudaMemcpy(ctx->d_gsz.p, ctx->pair_gsz.data(), np * sizeof(int), cudaMemcpyHostToDevice));
+  CUCHK(cudaMemcpy(ctx->d_gpoff.p, gpoff.data(), np * sizeof(int), cudaMemcpyHostToDevice));
+  CUCHK(cudaMemcpy(ctx->d_gnp.p, gnp.data(), np * sizeof(int), cudaMemcpyHostToDevice));
+  CUCHK(cudaMemcpy(ctx->d_gwoff.p, gwoff.data(), np * sizeof(int), cudaMemcpyHostToDevice));
+  if (!prim.empty())
+    CUCHK(cudaMemcpy(ctx->d_gprim.p, prim.data(), prim.size() * sizeof(PrimPair), cudaMemcpyHostToDevice));
+  if (!w.empty()) CUCHK(cudaMemcpy(ctx->d_gw.p, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice));
+  if (ng) {
+    CUCHK(cudaMemcpy(ctx->d_glead.p, ctx->glead.data(), ng * sizeof(int), cudaMemcpyHostToDevice));
+    CUCHK(cudaMemcpy(ctx->d_gQ.p, ctx->gQ.data(), ng * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  ctx->group_prim_pairs = (long long)prim.size();
+  return CQG_OK;
+}
+
+// The active block table: bra-group tasks for the sibling classes, or pair tasks for all.
+static void select_block_table(cqg_ctx *ctx) {
+  ctx->bt = ctx->siblings ? ctx->bt_group : ctx->bt_pair;
+  ctx->ntask = ctx->siblings ? ctx->ntask_group : ctx->ntask_pair;
+}
+
+// Class-block tables: pair tasks for every class (bt_pair), and bra-group tasks for the
+// sibling classes (bt_group); then the active one.  The per-task count and offset arrays
+// are sized for the larger of the two.
+static cqg_status build_block_tables(cqg_ctx *ctx) {
+  for (int mode = 0; mode < 2; ++mode) {
+    BlockTable &bt = mode ? ctx->bt_group : ctx->bt_pair;
+    memset(&bt, 0, sizeof(bt));
+    int task = 0;
+    for (int k = 0; k < CQG_NQC; ++k) {
+      int i, j;
+      qclass_split(k, i, j);
+      bt.task_beg[k] = task;
+      bt.bra_beg[k] = ctx->pc_beg[i];
+      bt.ket_beg[k] = ctx->pc_beg[j];
+      bt.ket_n[k] = ctx->pc_beg[j + 1] - ctx->pc_beg[j];
+      bt.ket_class[k] = j;
+      bt.diag[k] = (i == j);
+      bt.grouped[k] = mode == 1 && class_grouped(k) && ctx->sibling_min[k] > 0;
+      bt.gbra_beg[k] = ctx->gc_beg[i];
+      bt.min_members[k] = ctx->sibling_min[k];
+      task += bt.grouped[k] ? ctx->gc_beg[i + 1] - ctx->gc_beg[i] : ctx->pc_beg[i + 1] - ctx->pc_beg[i];
+    }
+    bt.task_beg[CQG_NQC] = task;
+    bt.nblk = CQG_NQC;
+    (mode ? ctx->ntask_group : ctx->ntask_pair) = task;
+  }
+  select_block_table(ctx);
+  const size_t task = (size_t)std::max(ctx->ntask_pair, ctx->ntask_group);
+  size_t scan_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (long long *)nullptr, (long long *)nullptr,
+                                std::max<int>(kListParts * (int)task, 1));
+  if (ctx->d_cnt.reserve(kListParts * task + 1) || ctx->d_off.reserve(kListParts * task + 1) ||
+      ctx->d_scan_tmp.reserve(scan_bytes + 16))
+    return CQG_ERR_OOM;
+  return CQG_OK;
+}
+
+
 // Launchers of every quartet class (eri_part.cu, a share per translation unit), merged
 // into one table per precision.
-#define CQG_SHARE_DECL(k) const eri_launcher *cqg_eri_part_table_##k(int fp32);
+#define CQG_SHARE_DECL(k)                                 \
+  const eri_launcher *cqg_eri_part_table_##k(int fp32); \
+  const eri_launcher *cqg_eri_part_gc_table_##k(int fp32);
 CQG_SHARE_DECL(0)
 CQG_SHARE_DECL(1)
 CQG_SHARE_DECL(2)
@@ -141,18 +319,36 @@ static const eri_launcher *cqg_eri_part_table(int part, int fp32) {
     default: return cqg_eri_part_table_7(fp32);
   }
 }
+static const eri_launcher *cqg_eri_part_gc_table(int part, int fp32) {
+  switch (part) {
+    case 0: return cqg_eri_part_gc_table_0(fp32);
+    case 1: return cqg_eri_part_gc_table_1(fp32);
+    case 2: return cqg_eri_part_gc_table_2(fp32);
+    case 3: return cqg_eri_part_gc_table_3(fp32);
+    case 4: return cqg_eri_part_gc_table_4(fp32);
+    case 5: return cqg_eri_part_gc_table_5(fp32);
+    case 6: return cqg_eri_part_gc_table_6(fp32);
+    default: return cqg_eri_part_gc_table_7(fp32);
+  }
+}
+// launcher of every work list vb = part * CQG_NQC + class: the class kernels (FP64, FP32)
+// for the pair entries, the sibling-group kernels (FP64, FP32; null for the other classes)
+// for the sibling entries
 struct EriTables {
-  eri_launcher t64[CQG_NQC], t32[CQG_NQC];
+  eri_launcher t[CQG_NLIST];
   EriTables() {
     for (int k = 0; k < CQG_NQC; ++k) {
-      t64[k] = cqg_eri_part_table(k % CQG_NPART, 0)[k];
-      t32[k] = cqg_eri_part_table(k % CQG_NPART, 1)[k];
+      t[k] = cqg_eri_part_table(k % CQG_NPART, 0)[k];
+      t[CQG_NQC + k] = cqg_eri_part_table(k % CQG_NPART, 1)[k];
+      t[2 * CQG_NQC + k] = cqg_eri_part_gc_table(k % CQG_NPART, 0)[k];
+      t[3 * CQG_NQC + k] = cqg_eri_part_gc_table(k % CQG_NPART, 1)[k];
     }
   }
 };
 static const EriTables kEriTables;
-static const eri_launcher *const kEriLaunch = kEriTables.t64;
-static const eri_launcher *const kEriLaunch32 = kEriTables.t32;
+static const eri_launcher *const kEriLaunch = kEriTables.t;      // FP64 class lists
+static const eri_launcher *const kEriLaunch32 = kEriTables.t + CQG_NQC;
+static inline eri_launcher list_launcher(int vb) { return kEriTables.t[vb]; }
 
 extern "C" {
 
@@ -170,6 +366,13 @@ const char *cqg_status_string(cqg_status s) {
     case CQG_ERR_UNSUPPORTED: return "unsupported input";
   }
   return "unknown status";
+}
+
+int cqg_schedule_lists(void) { return CQG_NLIST; }
+
+int cqg_list_class(int b) {
+  if (b < 0 || b >= CQG_NLIST) return -1;
+  return b % CQG_NQC;
 }
 
 const char *cqg_class_name(int k) {
@@ -207,7 +410,8 @@ cqg_status cqg_create(cqg_ctx **out, int device) {
     delete ctx;
     return CQG_ERR_CUDA;
   }
-  for (int i = 0; i < 4 + 2 * 55 + 2; ++i) cudaEventCreate(&ctx->ev[i]);
+  for (int i = 0; i < 4 + 2 * CQG_NQC + 2; ++i) cudaEventCreate(&ctx->ev[i]);
+  for (int k = 0; k < CQG_NQC; ++k) ctx->sibling_min[k] = default_sibling_min(k);
   ctx->events = true;
   cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
   *out = ctx;
@@ -229,8 +433,11 @@ cqg_status cqg_destroy(cqg_ctx *ctx) {
   ctx->d_cnt.release(); ctx->d_off.release(); ctx->d_range.release(); ctx->d_scan_tmp.release();
   ctx->d_qhead.release();
   ctx->d_qlist.release(); ctx->d_G.release(); ctx->d_X.release(); ctx->d_AX.release(); ctx->d_Gscratch.release();
+  ctx->d_molgbk.release(); ctx->d_gsz.release(); ctx->d_gpoff.release(); ctx->d_gnp.release(); ctx->d_gwoff.release();
+  ctx->d_glead.release(); ctx->d_pair_Qc.release(); ctx->d_gQ.release(); ctx->d_gw.release(); ctx->d_gprim.release();
+  ctx->d_qmask.release();
   if (ctx->events)
-    for (int i = 0; i < 4 + 2 * 55 + 2; ++i) cudaEventDestroy(ctx->ev[i]);
+    for (int i = 0; i < 4 + 2 * CQG_NQC + 2; ++i) cudaEventDestroy(ctx->ev[i]);
   delete ctx;
   return CQG_OK;
 }
@@ -431,19 +638,58 @@ cqg_status cqg_set_basis_batch(cqg_ctx *ctx, int nmol, const int *nshell_per_mol
   } else {
     ctx->Qmat.clear();
   }
-  // sort each class by (molecule, primitive-count bucket, Q descending), stable, and
-  // rebuild with primitive-pair screening; per (molecule, class) bucket starts -> molbk
-  std::vector<int> npscr(ctx->pair_sh.size());
+  // Sibling groups per pair class (csrc/siblings.h), their largest Q and the size of the
+  // union of their members' screened primitive pairs.
+  const int npairs = (int)ctx->pair_sh.size();
+  const std::vector<int> fam = cqg_sib::shell_families(nshell, L, nprim, ctx->hpoff.data(), alpha, centers,
+                                                       ctx->hshmol.data());
+  std::vector<int> pgid(npairs), prank(npairs), gnp_of(npairs), gsz_of(npairs);   // *_of: by group id
+  std::vector<double> gq_of(npairs, 0.0);
   {
+    int gbase = 0;
+    std::vector<int> pa, pb, gid, rank;
+    for (int c = 0; c < CQG_NPC; ++c) {
+      const int b0 = ctx->pc_beg[c], n = ctx->pc_beg[c + 1] - b0;
+      pa.resize(n);
+      pb.resize(n);
+      for (int k = 0; k < n; ++k) {
+        pa[k] = ctx->pair_sh[b0 + k].x;
+        pb[k] = ctx->pair_sh[b0 + k].y;
+      }
+      const int cap = sibling_cap(kPairClass[c][0], kPairClass[c][1]);
+      const int ng = cqg_sib::pair_groups(n, pa.data(), pb.data(), L, fam, cap, gid, rank);
+      for (int k = 0; k < n; ++k) {
+        pgid[b0 + k] = gbase + gid[k];
+        prank[b0 + k] = rank[k];
+      }
+      gbase += ng;
+    }
+    std::vector<std::vector<int>> members(gbase);
+    for (int i = 0; i < npairs; ++i) members[pgid[i]].push_back(i);
     std::vector<PrimPair> tmp;
-    for (size_t i = 0; i < ctx->pair_sh.size(); ++i) {
+    std::vector<double> w;
+    for (int g = 0; g < gbase; ++g) {
+      double q = 0.0;
+      for (int i : members[g]) q = std::max(q, ctx->pair_Q[i]);
+      gq_of[g] = q;
+      gsz_of[g] = (int)members[g].size();
       tmp.clear();
-      pair_prims(ctx, ctx->pair_sh[i].x, ctx->pair_sh[i].y, 1e-24, tmp);
-      npscr[i] = (int)tmp.size();
+      w.clear();
+      group_prims(ctx, members[g].data(), (int)members[g].size(), 1, 1e-24, fam, tmp, w);
+      gnp_of[g] = (int)tmp.size();
     }
   }
+  // Sort each class by (molecule, bucket of the group, group Q descending, group, member),
+  // stable; the bucket is (one member or more, primitive-count bucket).  The members of a
+  // group become consecutive pairs led by the first, and Qc (the group's Q) is
+  // non-increasing within each bucket.  Per (molecule, class) bucket starts -> molbk (pair
+  // index) and molgbk (group index).
+  auto bucket_of = [&](int i) {
+    return (gsz_of[pgid[i]] > 1 ? CQG_NPBUCKET : 0) + prim_bucket(gnp_of[pgid[i]]);
+  };
   const int NB1 = CQG_NBUCKET + 1;
-  std::vector<int> molbk((size_t)nmol * CQG_NPC * NB1, 0);
+  std::vector<int> molbk((size_t)nmol * CQG_NPC * NB1, 0), molgbk((size_t)nmol * CQG_NPC * NB1, 0);
+  std::vector<int> new_gid(npairs);
   for (int c = 0; c < CQG_NPC; ++c) {
     int b0 = ctx->pc_beg[c], b1 = ctx->pc_beg[c + 1];
     std::vector<int> idx(b1 - b0);
@@ -451,14 +697,17 @@ cqg_status cqg_set_basis_batch(cqg_ctx *ctx, int nmol, const int *nshell_per_mol
     std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
       int mx = ctx->hshmol[ctx->pair_sh[x].x], my = ctx->hshmol[ctx->pair_sh[y].x];
       if (mx != my) return mx < my;
-      int bx = prim_bucket(npscr[x]), by = prim_bucket(npscr[y]);
+      int bx = bucket_of(x), by = bucket_of(y);
       if (bx != by) return bx < by;
-      return ctx->pair_Q[x] > ctx->pair_Q[y];
+      const double qx = gq_of[pgid[x]], qy = gq_of[pgid[y]];
+      if (qx != qy) return qx > qy;
+      if (pgid[x] != pgid[y]) return pgid[x] < pgid[y];
+      return prank[x] < prank[y];
     });
     // bucket starts per molecule: first index of (m, bk); empty buckets start where the next begins
     std::vector<int> first((size_t)nmol * NB1, -1);
     for (int k = 0; k < (int)idx.size(); ++k) {
-      const int m = ctx->hshmol[ctx->pair_sh[idx[k]].x], bk = prim_bucket(npscr[idx[k]]);
+      const int m = ctx->hshmol[ctx->pair_sh[idx[k]].x], bk = bucket_of(idx[k]);
       if (first[(size_t)m * NB1 + bk] < 0) first[(size_t)m * NB1 + bk] = b0 + k;
     }
     int next = b1;
@@ -474,46 +723,63 @@ cqg_status cqg_set_basis_batch(cqg_ctx *ctx, int nmol, const int *nshell_per_mol
     for (int bk = 0; bk <= CQG_NBUCKET; ++bk) ctx->bucket_beg[c][bk] = molbk[(size_t)c * NB1 + bk];
     std::vector<int2> sh2;
     std::vector<double> q2;
+    std::vector<int> g2;
     for (int i : idx) {
       sh2.push_back(ctx->pair_sh[i]);
       q2.push_back(ctx->pair_Q[i]);
+      g2.push_back(pgid[i]);
     }
     std::copy(sh2.begin(), sh2.end(), ctx->pair_sh.begin() + b0);
     std::copy(q2.begin(), q2.end(), ctx->pair_Q.begin() + b0);
+    std::copy(g2.begin(), g2.end(), new_gid.begin() + b0);
   }
-  if (ctx->d_molbk.reserve(molbk.size())) return CQG_ERR_OOM;
+  // group index space in pair order: leaders, group sizes, Qc, bucket starts by group
+  ctx->pair_gsz.assign(npairs, 0);
+  ctx->pair_Qc.assign(npairs, 0.0);
+  ctx->glead.clear();
+  ctx->gQ.clear();
+  {
+    std::vector<int> pair_group(npairs);
+    for (int i = 0; i < npairs; ++i) {
+      if (i == 0 || new_gid[i] != new_gid[i - 1]) {
+        ctx->glead.push_back(i);
+        ctx->gQ.push_back(gq_of[new_gid[i]]);
+      }
+      pair_group[i] = (int)ctx->glead.size() - 1;
+      ctx->pair_gsz[ctx->glead.back()] += 1;
+      ctx->pair_Qc[i] = gq_of[new_gid[i]];
+    }
+    const int ngroups = (int)ctx->glead.size();
+    for (int c = 0; c <= CQG_NPC; ++c) {
+      const int pb = ctx->pc_beg[c];
+      ctx->gc_beg[c] = pb < npairs ? pair_group[pb] : ngroups;
+    }
+    for (size_t k = 0; k < molbk.size(); ++k) molgbk[k] = molbk[k] < npairs ? pair_group[molbk[k]] : ngroups;
+  }
+  if (ctx->d_molbk.reserve(molbk.size()) || ctx->d_molgbk.reserve(molgbk.size())) return CQG_ERR_OOM;
   CUCHK(cudaMemcpy(ctx->d_molbk.p, molbk.data(), molbk.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CUCHK(cudaMemcpy(ctx->d_molgbk.p, molgbk.data(), molgbk.size() * sizeof(int), cudaMemcpyHostToDevice));
   st = upload_pairs(ctx, 1e-24);
   if (st != CQG_OK) return st;
-  // class-block table
-  BlockTable &bt = ctx->bt;
-  memset(&bt, 0, sizeof(bt));
-  int task = 0;
-  for (int k = 0; k < CQG_NQC; ++k) {
-    int i, j;
-    qclass_split(k, i, j);
-    bt.task_beg[k] = task;
-    bt.bra_beg[k] = ctx->pc_beg[i];
-    bt.ket_beg[k] = ctx->pc_beg[j];
-    bt.ket_n[k] = ctx->pc_beg[j + 1] - ctx->pc_beg[j];
-    bt.ket_class[k] = j;
-    bt.diag[k] = (i == j);
-    task += ctx->pc_beg[i + 1] - ctx->pc_beg[i];
+  st = upload_groups(ctx, fam, 1e-24);
+  if (st != CQG_OK) return st;
+  {
+    cqg_status bst = build_block_tables(ctx);
+    if (bst != CQG_OK) return bst;
   }
-  bt.task_beg[CQG_NQC] = task;
-  bt.nblk = CQG_NQC;
-  ctx->ntask = task;
+  const int task = std::max(ctx->ntask_pair, ctx->ntask_group);
   for (int k = 0; k < CQG_NQC; ++k) {
     int i, j;
     qclass_split(k, i, j);
     ctx->class_possible[k] = ctx->pc_beg[i + 1] > ctx->pc_beg[i] && ctx->pc_beg[j + 1] > ctx->pc_beg[j];
   }
   size_t scan_bytes = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (long long *)nullptr, (long long *)nullptr, std::max(2 * task, 1));
-  if (ctx->d_cnt.reserve(2 * task + 1) || ctx->d_off.reserve(2 * task + 1) || ctx->d_range.reserve(4 * CQG_NQC) ||
-      ctx->d_qhead.reserve(2 * CQG_NQC + 1) ||
+  cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (long long *)nullptr, (long long *)nullptr,
+                                std::max(kListParts * task, 1));
+  if (ctx->d_cnt.reserve(kListParts * (size_t)task + 1) || ctx->d_off.reserve(kListParts * (size_t)task + 1) ||
+      ctx->d_range.reserve(2 * CQG_NLIST) || ctx->d_qhead.reserve(CQG_NLIST + 1) ||
       ctx->d_scan_tmp.reserve(scan_bytes + 16) || ctx->d_M.reserve(2 * (size_t)std::max(ctx->Mtotal, 1LL)) ||
-      ctx->d_Mmax.reserve(1) || ctx->d_flags.reserve(4) || ctx->d_blkacc.reserve(4 * CQG_NQC) ||
+      ctx->d_Mmax.reserve(1) || ctx->d_flags.reserve(4) || ctx->d_blkacc.reserve(kBlkAcc * CQG_NQC) ||
       ctx->d_Mpair.reserve(std::max<size_t>(ctx->pair_sh.size(), 1)))
     return CQG_ERR_OOM;
   return CQG_OK;
@@ -532,8 +798,11 @@ cqg_status cqg_get_schwarz(cqg_ctx *ctx, double *Q) {
 }
 
 // Whether quartet class k goes through the class-fused kernel of `tier` (0: none).
-static bool class_fused(int tier, int k) {
-  if (tier == 0) return false;
+// whether work list vb (part * CQG_NQC + class) goes through the class-fused kernel of
+// `tier` (the pair entries of the tier's classes; a class index k < CQG_NQC is its FP64 list)
+static bool class_fused(int tier, int vb) {
+  if (tier == 0 || vb >= 2 * CQG_NQC) return false;
+  const int k = vb % CQG_NQC;
   int i, j;
   qclass_split(k, i, j);
   return cqg_fused_member(tier, kPairClass[i][0], kPairClass[i][1], kPairClass[j][0], kPairClass[j][1]);
@@ -552,14 +821,16 @@ static cqg_status autotune_shapes(cqg_ctx *ctx, const long long *crange, cudaStr
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  for (int vb = 0; vb < 2 * CQG_NQC; ++vb) {
+  for (int vb = 0; vb < CQG_NLIST; ++vb) {
     const long long n = crange[2 * vb + 1] - crange[2 * vb];
-    if (n <= 0) continue;
+    if (n <= 0 || !list_launcher(vb)) continue;
     const int k = vb % CQG_NQC;
+    const bool sibling = vb >= 2 * CQG_NQC;
     int i, j;
     qclass_split(k, i, j);
     const int la = kPairClass[i][0], lb = kPairClass[i][1], lc = kPairClass[j][0], ld = kPairClass[j][1];
-    const bool warp = is_warp_class(la, lb, lc, ld), both = is_variant_class(la, lb, lc, ld);
+    const bool warp = !sibling && is_warp_class(la, lb, lc, ld);
+    const bool both = !sibling && is_variant_class(la, lb, lc, ld);
     struct Shape {
       int cta, wpb, qpw, var;
     };
@@ -596,7 +867,7 @@ static cqg_status autotune_shapes(cqg_ctx *ctx, const long long *crange, cudaStr
       for (int rep = 0; rep < (ci < 0 ? 1 : reps); ++rep) {
         CUCHK(cudaMemsetAsync(ctx->d_qhead.p + vb, 0, sizeof(unsigned long long), st));
         cudaEventRecord(e0, st);
-        cudaError_t e = (vb < CQG_NQC ? kEriLaunch[k] : kEriLaunch32[k])(ctx, vb, m, st, scratch);
+        cudaError_t e = list_launcher(vb)(ctx, vb, m, st, scratch);
         cudaEventRecord(e1, st);
         if (e != cudaSuccess) {
           cudaEventDestroy(e0);
@@ -626,22 +897,21 @@ static cqg_status autotune_shapes(cqg_ctx *ctx, const long long *crange, cudaStr
   // launches of the rest, and as the tier-2 fused kernel; full lists, each timed after one
   // untimed run; the fastest is kept.
   bool any = false;
-  for (int vb = 0; vb < 2 * CQG_NQC; ++vb)
-    if (crange[2 * vb + 1] > crange[2 * vb] && class_fused(2, vb % CQG_NQC)) any = true;
+  for (int vb = 0; vb < CQG_NLIST; ++vb)
+    if (crange[2 * vb + 1] > crange[2 * vb] && class_fused(2, vb)) any = true;
   if (any) {
     float best = 1e30f;
     int pick = 0;
     for (int tier = 0; tier <= 2; ++tier) {
       float t = 1e30f;
       for (int rep = 0; rep < 2; ++rep) {
-        CUCHK(cudaMemsetAsync(ctx->d_qhead.p, 0, 2 * CQG_NQC * sizeof(unsigned long long), st));
+        CUCHK(cudaMemsetAsync(ctx->d_qhead.p, 0, CQG_NLIST * sizeof(unsigned long long), st));
         cudaEventRecord(e0, st);
         cudaError_t e = tier ? cqg_launch_fused(ctx, tier, st, scratch) : cudaSuccess;
-        for (int vb = 0; vb < 2 * CQG_NQC && e == cudaSuccess; ++vb) {
-          const int k = vb % CQG_NQC;
+        for (int vb = 0; vb < CQG_NLIST && e == cudaSuccess; ++vb) {
           const long long n = crange[2 * vb + 1] - crange[2 * vb];
-          if (n <= 0 || !class_fused(2, k) || class_fused(tier, k)) continue;
-          e = (vb < CQG_NQC ? kEriLaunch[k] : kEriLaunch32[k])(ctx, vb, n, st, scratch);
+          if (n <= 0 || !class_fused(2, vb) || class_fused(tier, vb)) continue;
+          e = list_launcher(vb)(ctx, vb, n, st, scratch);
         }
         cudaEventRecord(e1, st);
         if (e != cudaSuccess) {
@@ -677,7 +947,8 @@ static cqg_status contract_graph(cqg_ctx *ctx, int ngroups, const double *const 
                                  int ldax, cudaStream_t st) {
   const Mols mols = make_mols(ctx);
   const size_t gsize = ctx->nmol > 1 ? (size_t)ctx->packed : (size_t)ctx->nbf * ctx->nbf;
-  if ((size_t)ngroups * gsize > ctx->d_G.n || (size_t)ctx->graph_capacity > ctx->d_qlist.n) {
+  if ((size_t)ngroups * gsize > ctx->d_G.n || (size_t)ctx->graph_capacity > ctx->d_qlist.n ||
+      (size_t)ctx->graph_capacity > ctx->d_qmask.n) {
     ctx->err = "graph mode: buffers were not reserved for this call (cqg_set_graph_mode)";
     return CQG_ERR_STATE;
   }
@@ -687,7 +958,7 @@ static cqg_status contract_graph(cqg_ctx *ctx, int ngroups, const double *const 
   const double cut32 = ctx->policy == CQG_PREC_MIXED ? ctx->fp32_cutoff : 0.0;
   CUCHK(cudaMemsetAsync(ctx->d_flags.p, 0, 4 * sizeof(int), st));
   CUCHK(cudaMemsetAsync(ctx->d_Mmax.p, 0, sizeof(double), st));
-  CUCHK(cudaMemsetAsync(ctx->d_blkacc.p, 0, 4 * CQG_NQC * sizeof(unsigned long long), st));
+  CUCHK(cudaMemsetAsync(ctx->d_blkacc.p, 0, kBlkAcc * CQG_NQC * sizeof(unsigned long long), st));
   CUCHK(cudaMemsetAsync(ctx->d_G.p, 0, (size_t)ngroups * gsize * sizeof(double), st));
   {
     dim3 g((ctx->max_nsh + 127) / 128, ctx->max_nsh, ctx->nmol);
@@ -701,15 +972,17 @@ static cqg_status contract_graph(cqg_ctx *ctx, int ngroups, const double *const 
   Pairs P = make_pairs(ctx);
   const int nb = (ctx->ntask + 7) / 8;
   k_quartets<false><<<nb, 256, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, ctx->d_Mpair.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
-                                         ctx->thresh, cut32, ctx->d_cnt.p, nullptr, nullptr, ctx->d_blkacc.p, 0, 0, 0,
-                                         0);
+                                         ctx->thresh, cut32, ctx->d_cnt.p, nullptr, nullptr, nullptr, ctx->d_blkacc.p,
+                                         0, 0, 0, 0);
   size_t scan_bytes = ctx->d_scan_tmp.n;
-  CUCHK(cub::DeviceScan::ExclusiveSum(ctx->d_scan_tmp.p, scan_bytes, ctx->d_cnt.p, ctx->d_off.p, 2 * ctx->ntask, st));
-  k_block_ranges<<<1, 128, 0, st>>>(ctx->bt, ctx->ntask, ctx->d_cnt.p, ctx->d_off.p, ctx->d_range.p,
+  CUCHK(cub::DeviceScan::ExclusiveSum(ctx->d_scan_tmp.p, scan_bytes, ctx->d_cnt.p, ctx->d_off.p,
+                                      kListParts * ctx->ntask, st));
+  k_block_ranges<<<1, kRangeThreads, 0, st>>>(ctx->bt, ctx->ntask, ctx->d_cnt.p, ctx->d_off.p, ctx->d_range.p,
                                     ctx->graph_capacity, ctx->d_flags.p);
   k_quartets<true><<<nb, 256, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, ctx->d_Mpair.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
-                                        ctx->thresh, cut32, nullptr, ctx->d_off.p, ctx->d_qlist.p, nullptr, 0,
-                                        2LL * ctx->ntask, 0, ctx->graph_capacity);
+                                        ctx->thresh, cut32, nullptr, ctx->d_off.p, ctx->d_qlist.p, ctx->d_qmask.p,
+                                        nullptr, 0,
+                                        (long long)kListParts * ctx->ntask, 0, ctx->graph_capacity);
   CUCHK(cudaGetLastError());
   DigestGroups dg;
   memset(&dg, 0, sizeof(dg));
@@ -724,7 +997,7 @@ static cqg_status contract_graph(cqg_ctx *ctx, int ngroups, const double *const 
     dg.sJ[g] = sJ[g];
     dg.sK[g] = sK[g];
   }
-  CUCHK(cudaMemsetAsync(ctx->d_qhead.p, 0, 2 * CQG_NQC * sizeof(unsigned long long), st));
+  CUCHK(cudaMemsetAsync(ctx->d_qhead.p, 0, CQG_NLIST * sizeof(unsigned long long), st));
   int launches = 7;   // block norms, max, pair norms, list count, scan, ranges, list fill
   if (ctx->fused_tier) {
     cudaError_t e = cqg_launch_fused(ctx, ctx->fused_tier, st, dg);
@@ -734,14 +1007,13 @@ static cqg_status contract_graph(cqg_ctx *ctx, int ngroups, const double *const 
       return CQG_ERR_CUDA;
     }
   }
-  for (int k = 0; k < CQG_NQC; ++k) {
-    if (!ctx->class_possible[k] || class_fused(ctx->fused_tier, k)) continue;
-    cudaError_t e = kEriLaunch[k](ctx, k, -1, st, dg);
+  for (int vb = 0; vb < CQG_NLIST; ++vb) {
+    const int k = vb % CQG_NQC, part = vb / CQG_NQC;
+    if (!ctx->class_possible[k] || class_fused(ctx->fused_tier, vb) || !list_launcher(vb)) continue;
+    if ((part & 1) && ctx->policy != CQG_PREC_MIXED) continue;   // FP32 lists are empty
+    if (part >= 2 && !ctx->bt.grouped[k]) continue;               // no sibling entries
+    cudaError_t e = list_launcher(vb)(ctx, vb, -1, st, dg);
     ++launches;
-    if (e == cudaSuccess && ctx->policy == CQG_PREC_MIXED) {
-      e = kEriLaunch32[k](ctx, CQG_NQC + k, -1, st, dg);
-      ++launches;
-    }
     if (e != cudaSuccess) {
       ctx->err = std::string("eri kernel ") + cqg_class_name(k) + ": " + cudaGetErrorString(e);
       return CQG_ERR_CUDA;
@@ -772,7 +1044,7 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
   for (int i = 0; i < nx_all; ++i) xl.X[i] = Xall[i];
   CUCHK(cudaMemsetAsync(ctx->d_flags.p, 0, 4 * sizeof(int), st));
   CUCHK(cudaMemsetAsync(ctx->d_Mmax.p, 0, sizeof(double), st));
-  CUCHK(cudaMemsetAsync(ctx->d_blkacc.p, 0, 4 * CQG_NQC * sizeof(unsigned long long), st));
+  CUCHK(cudaMemsetAsync(ctx->d_blkacc.p, 0, kBlkAcc * CQG_NQC * sizeof(unsigned long long), st));
   const double cut32 = ctx->policy == CQG_PREC_MIXED ? ctx->fp32_cutoff : 0.0;
   ctx->launches = 0;
   {
@@ -795,17 +1067,19 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     int nb = (ctx->ntask + wpb - 1) / wpb;
     k_quartets<false><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, ctx->d_Mpair.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
                                             ctx->thresh,
-                                            cut32, ctx->d_cnt.p, nullptr, nullptr, ctx->d_blkacc.p, 0, 0, 0, 0);
+                                            cut32, ctx->d_cnt.p, nullptr, nullptr, nullptr, ctx->d_blkacc.p, 0, 0, 0,
+                                            0);
     CUCHK(cudaGetLastError());
     size_t scan_bytes = ctx->d_scan_tmp.n;
-    CUCHK(cub::DeviceScan::ExclusiveSum(ctx->d_scan_tmp.p, scan_bytes, ctx->d_cnt.p, ctx->d_off.p, 2 * ctx->ntask, st));
-    k_block_ranges<<<1, 128, 0, st>>>(ctx->bt, ctx->ntask, ctx->d_cnt.p, ctx->d_off.p, ctx->d_range.p, LLONG_MAX,
+    CUCHK(cub::DeviceScan::ExclusiveSum(ctx->d_scan_tmp.p, scan_bytes, ctx->d_cnt.p, ctx->d_off.p,
+                                      kListParts * ctx->ntask, st));
+    k_block_ranges<<<1, kRangeThreads, 0, st>>>(ctx->bt, ctx->ntask, ctx->d_cnt.p, ctx->d_off.p, ctx->d_range.p, LLONG_MAX,
                                       ctx->d_flags.p);
     CUCHK(cudaGetLastError());
     ctx->launches += 2;
   }
-  long long hr[4 * CQG_NQC];
-  unsigned long long hacc[4 * CQG_NQC];
+  long long hr[2 * CQG_NLIST];
+  unsigned long long hacc[kBlkAcc * CQG_NQC];
   int hflags[4];
   CUCHK(cudaMemcpyAsync(hr, ctx->d_range.p, sizeof(hr), cudaMemcpyDeviceToHost, st));
   CUCHK(cudaMemcpyAsync(hacc, ctx->d_blkacc.p, sizeof(hacc), cudaMemcpyDeviceToHost, st));
@@ -819,13 +1093,14 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     ctx->err = "input matrix is not symmetric; this engine contracts real symmetric X only";
     return CQG_ERR_UNSUPPORTED;
   }
-  long long total = hr[4 * CQG_NQC - 1];
-  // The list is [FP64 part of every task][FP32 part of every task] ("virtual tasks"
-  // 0 .. 2 ntask).  It is filled and consumed in chunks of at most `list_budget` quartets.
+  long long total = hr[2 * CQG_NLIST - 1];
+  // The list is [FP64 pair entries of every task][FP32 pair entries][FP64 sibling
+  // entries][FP32 sibling entries] ("virtual tasks" 0 .. 4 ntask).  It is filled and
+  // consumed in chunks of at most `list_budget` entries.
   const long long budget = std::max<long long>(ctx->list_budget, 1);
   std::vector<long long> chunk_vt;   // chunk boundaries in virtual tasks
   std::vector<long long> hoff, hcnt;
-  const long long nvt = 2LL * ctx->ntask;
+  const long long nvt = (long long)kListParts * ctx->ntask;
   if (total <= budget) {
     chunk_vt = {0, nvt};
   } else {
@@ -852,7 +1127,8 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
       cap = std::max(cap, hoff[v1 - 1] + hcnt[v1 - 1] - hoff[v0]);
     }
   }
-  if (ctx->d_qlist.reserve((size_t)std::max<long long>(cap, 1)) != cudaSuccess) {
+  if (ctx->d_qlist.reserve((size_t)std::max<long long>(cap, 1)) != cudaSuccess ||
+      ctx->d_qmask.reserve((size_t)std::max<long long>(cap, 1)) != cudaSuccess) {
     ctx->err = "quartet list allocation failed";
     return CQG_ERR_OOM;
   }
@@ -877,28 +1153,32 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
   ctx->stats.ms_fused = 0.0;
   ctx->stats.fused_tier = ctx->fused_tier;
   double mflops = 0, mflops32 = 0;
-  long long nprimq = 0, nq32 = 0;
+  long long nprimq = 0, nq32 = 0, nquart = 0;
   for (int k = 0; k < CQG_NQC; ++k) {
-    const long long n64 = hr[2 * k + 1] - hr[2 * k];
-    const long long n32 = hr[2 * (CQG_NQC + k) + 1] - hr[2 * (CQG_NQC + k)];
-    ctx->stats.class_quartets[k] = n64 + n32;
+    // contracted quartets (a sibling-group entry of the list holds several)
+    const int b = k;
+    const long long n64 = (long long)hacc[kBlkAcc * b + 4];
+    const long long n32 = (long long)hacc[kBlkAcc * b + 5];
+    ctx->stats.class_quartets[k] += n64 + n32;
     nq32 += n32;
+    nquart += n64 + n32;
     int i, j;
     qclass_split(k, i, j);
     const int la = kPairClass[i][0], lb = kPairClass[i][1], lc = kPairClass[j][0], ld = kPairClass[j][1];
     const double fp = md_v1_prim_flops(la, lb, lc, ld), fd = md_v1_digest_flops(la, lb, lc, ld);
-    mflops += (double)hacc[4 * k] * fp + (double)n64 * fd;
-    mflops32 += (double)hacc[4 * k + 2] * fp + (double)n32 * fd;
-    nprimq += (long long)(hacc[4 * k + 1] + hacc[4 * k + 3]);
+    mflops += (double)hacc[kBlkAcc * b] * fp + (double)n64 * fd;
+    mflops32 += (double)hacc[kBlkAcc * b + 2] * fp + (double)n32 * fd;
+    nprimq += (long long)(hacc[kBlkAcc * b + 1] + hacc[kBlkAcc * b + 3]);
   }
   bool first_chunk = true;
+  bool timed[CQG_NQC] = {false};
   for (size_t ch = 0; ch + 1 < chunk_vt.size(); ++ch) {
     const long long vt0 = chunk_vt[ch], vt1 = chunk_vt[ch + 1];
     long long obase = 0;
-    long long crange[4 * CQG_NQC];
+    long long crange[2 * CQG_NLIST];
     if (chunk_vt.size() > 2) {
       obase = hoff[vt0];
-      for (int vb = 0; vb < 2 * CQG_NQC; ++vb) {
+      for (int vb = 0; vb < CQG_NLIST; ++vb) {
         const int prec = vb / CQG_NQC, b = vb % CQG_NQC;
         long long t0 = (long long)prec * ctx->ntask + ctx->bt.task_beg[b];
         long long t1 = (long long)prec * ctx->ntask + ctx->bt.task_beg[b + 1];
@@ -913,15 +1193,16 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
       }
       CUCHK(cudaMemcpyAsync(ctx->d_range.p, crange, sizeof(crange), cudaMemcpyHostToDevice, st));
     } else {
-      for (int q = 0; q < 4 * CQG_NQC; ++q) crange[q] = hr[q];
+      for (int q = 0; q < 2 * CQG_NLIST; ++q) crange[q] = hr[q];
     }
     {
       int nthr = 256, wpb = nthr / 32;
       int nb = (ctx->ntask + wpb - 1) / wpb;
       k_quartets<true><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, ctx->d_Mpair.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
                                              ctx->thresh,
-                                             cut32, nullptr, ctx->d_off.p, ctx->d_qlist.p, nullptr, vt0, vt1, obase,
-                                             (long long)ctx->d_qlist.n);
+                                             cut32, nullptr, ctx->d_off.p, ctx->d_qlist.p, ctx->d_qmask.p, nullptr,
+                                             vt0, vt1, obase,
+                                             (long long)std::min(ctx->d_qlist.n, ctx->d_qmask.n));
       CUCHK(cudaGetLastError());
       ctx->launches += 1;
     }
@@ -932,7 +1213,7 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
       ctx->autotune_pending = 0;
     }
     // 3. ERI + digest per class, each list consumed through its work-queue head counter
-    CUCHK(cudaMemsetAsync(ctx->d_qhead.p, 0, 2 * CQG_NQC * sizeof(unsigned long long), st));
+    CUCHK(cudaMemsetAsync(ctx->d_qhead.p, 0, CQG_NLIST * sizeof(unsigned long long), st));
     if (ctx->fused_tier) {   // the fused tier's lists in one launch (its time: ms_fused)
       if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[4 + 2 * CQG_NQC], st));
       cudaError_t e = cqg_launch_fused(ctx, ctx->fused_tier, st, dg);
@@ -943,28 +1224,41 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
       if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[5 + 2 * CQG_NQC], st));
       ctx->launches += 1;
     }
-    for (int k = 0; k < CQG_NQC; ++k) {
-      if (class_fused(ctx->fused_tier, k)) continue;
-      const long long n64 = crange[2 * k + 1] - crange[2 * k];
-      const long long n32 = crange[2 * (CQG_NQC + k) + 1] - crange[2 * (CQG_NQC + k)];
-      if (n64 > 0) ctx->launches += 1;
-      if (n32 > 0) ctx->launches += 1;
-      if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[4 + 2 * k], st));
-      cudaError_t e = kEriLaunch[k](ctx, k, n64, st, dg);
-      if (e == cudaSuccess) e = kEriLaunch32[k](ctx, CQG_NQC + k, n32, st, dg);
-      if (e != cudaSuccess) {
-        ctx->err = std::string("eri kernel ") + cqg_class_name(k) + ": " + cudaGetErrorString(e);
-        return CQG_ERR_CUDA;
+    for (int k = 0; k < CQG_NQC; ++k) {   // the class's lists: pair entries FP64, FP32, sibling entries FP64, FP32
+      bool any_list = false;
+      for (int part = 0; part < kListParts; ++part) {
+        const int vb = part * CQG_NQC + k;
+        if (!class_fused(ctx->fused_tier, vb) && crange[2 * vb + 1] > crange[2 * vb]) any_list = true;
       }
-      if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[5 + 2 * k], st));
+      if (!any_list) continue;
+      if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[4 + 2 * k], st));
+      for (int part = 0; part < kListParts; ++part) {
+        const int vb = part * CQG_NQC + k;
+        const long long n = crange[2 * vb + 1] - crange[2 * vb];
+        if (n <= 0 || class_fused(ctx->fused_tier, vb)) continue;
+        if (!list_launcher(vb)) {
+          ctx->err = std::string("sibling entries for a class without the sibling form: ") + cqg_class_name(k);
+          return CQG_ERR_STATE;
+        }
+        ctx->launches += 1;
+        cudaError_t e = list_launcher(vb)(ctx, vb, n, st, dg);
+        if (e != cudaSuccess) {
+          ctx->err = std::string("eri kernel ") + cqg_class_name(k) + ": " + cudaGetErrorString(e);
+          return CQG_ERR_CUDA;
+        }
+      }
+      if (ctx->timing) {
+        CUCHK(cudaEventRecord(ctx->ev[5 + 2 * k], st));
+        timed[k] = true;
+      }
     }
-    if (ctx->timing) {   // per-class device time, summed over chunks
+    if (ctx->timing) {   // per-class device time (all lists of the class), summed over chunks
       CUCHK(cudaStreamSynchronize(st));
       for (int k = 0; k < CQG_NQC; ++k) {
         float ms = 0.f;
-        if (!class_fused(ctx->fused_tier, k) &&
-            cudaEventElapsedTime(&ms, ctx->ev[4 + 2 * k], ctx->ev[5 + 2 * k]) == cudaSuccess)
+        if (timed[k] && cudaEventElapsedTime(&ms, ctx->ev[4 + 2 * k], ctx->ev[5 + 2 * k]) == cudaSuccess)
           ctx->stats.class_ms[k] += ms;
+        timed[k] = false;
       }
       float ms = 0.f;
       if (ctx->fused_tier &&
@@ -982,7 +1276,13 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     ctx->launches += 1;
   }
   if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[3], st));
-  ctx->stats.quartets = total;
+  ctx->stats.quartets = nquart;
+  ctx->stats.list_entries = total;
+  ctx->stats.sibling_classes = 0;
+  for (int k = 0; k < CQG_NQC; ++k) {   // classes whose sibling-group lists had entries
+    const int v64 = 2 * CQG_NQC + k, v32 = 3 * CQG_NQC + k;
+    if (hr[2 * v64 + 1] > hr[2 * v64] || hr[2 * v32 + 1] > hr[2 * v32]) ctx->stats.sibling_classes |= 1LL << k;
+  }
   ctx->stats.quartets_fp32 = nq32;
   ctx->stats.model_flops = mflops + mflops32;
   ctx->stats.model_flops_fp32 = mflops32;
@@ -1317,7 +1617,8 @@ cqg_status cqg_set_graph_mode(cqg_ctx *ctx, long long capacity, int max_groups) 
   ctx->graph_capacity = capacity;
   if (capacity > 0) {
     const size_t gsize = ctx->nmol > 1 ? (size_t)ctx->packed : (size_t)ctx->nbf * ctx->nbf;
-    if (ctx->d_qlist.reserve((size_t)capacity) || ctx->d_G.reserve((size_t)std::max(max_groups, 1) * gsize)) {
+    if (ctx->d_qlist.reserve((size_t)capacity) || ctx->d_qmask.reserve((size_t)capacity) ||
+        ctx->d_G.reserve((size_t)std::max(max_groups, 1) * gsize)) {
       ctx->graph_capacity = 0;
       return CQG_ERR_OOM;
     }
@@ -1329,11 +1630,11 @@ cqg_status cqg_graph_status(cqg_ctx *ctx, long long *quartets, int *overflow, in
   if (!ctx) return CQG_ERR_BAD_ARG;
   CUCHK(cudaSetDevice(ctx->device));
   CUCHK(cudaDeviceSynchronize());
-  long long hr[4 * CQG_NQC];
+  long long hr[2 * CQG_NLIST];
   int fl[4];
   CUCHK(cudaMemcpy(fl, ctx->d_flags.p, sizeof(fl), cudaMemcpyDeviceToHost));
   CUCHK(cudaMemcpy(hr, ctx->d_range.p, sizeof(hr), cudaMemcpyDeviceToHost));
-  if (quartets) *quartets = hr[4 * CQG_NQC - 1];
+  if (quartets) *quartets = hr[2 * CQG_NLIST - 1];
   if (overflow) *overflow = fl[2];
   if (nonfinite) *nonfinite = fl[0];
   if (asymmetric) *asymmetric = fl[1];
@@ -1362,10 +1663,11 @@ cqg_status cqg_get_launch_shapes(cqg_ctx *ctx, int *cta_per_sm, int *warps_per_c
 cqg_status cqg_get_schedule(cqg_ctx *ctx, int *cta_per_sm, int *warps_per_cta, int *quartets_per_warp,
                             int *warp_form) {
   if (!ctx) return CQG_ERR_BAD_ARG;
-  for (int k = 0; k < 2 * CQG_NQC; ++k) {
+  for (int k = 0; k < CQG_NLIST; ++k) {
     int i, j;
     qclass_split(k % CQG_NQC, i, j);
-    const bool warp = is_warp_class(kPairClass[i][0], kPairClass[i][1], kPairClass[j][0], kPairClass[j][1]);
+    const bool warp = k < 2 * CQG_NQC &&
+                      is_warp_class(kPairClass[i][0], kPairClass[i][1], kPairClass[j][0], kPairClass[j][1]);
     if (cta_per_sm) cta_per_sm[k] = ctx->shape_cta[k];
     if (warps_per_cta) warps_per_cta[k] = ctx->shape_wpb[k];
     if (quartets_per_warp) quartets_per_warp[k] = ctx->shape_qpw[k];
@@ -1384,6 +1686,33 @@ cqg_status cqg_set_fusion(cqg_ctx *ctx, int tier) {
   return CQG_OK;
 }
 
+cqg_status cqg_set_siblings(cqg_ctx *ctx, int on) {
+  if (!ctx) return CQG_ERR_BAD_ARG;
+  ctx->siblings = on ? 1 : 0;
+  select_block_table(ctx);
+  return CQG_OK;
+}
+
+cqg_status cqg_set_sibling_min(cqg_ctx *ctx, int k, int min_members) {
+  if (!ctx) return CQG_ERR_BAD_ARG;
+  if (!class_grouped(k) || min_members < 0 || min_members == 1 || min_members > 16) {
+    ctx->err = "cqg_set_sibling_min: k is a sibling class and min_members is 0 (pair tasks) or 2..16";
+    return CQG_ERR_BAD_ARG;
+  }
+  ctx->sibling_min[k] = min_members;
+  if (ctx->nshell > 0) {   // rebuild the group-mode table: the class's tasks change
+    cqg_status st = build_block_tables(ctx);
+    if (st != CQG_OK) return st;
+  }
+  return CQG_OK;
+}
+
+cqg_status cqg_get_siblings(cqg_ctx *ctx, int *on) {
+  if (!ctx || !on) return CQG_ERR_BAD_ARG;
+  *on = ctx->siblings;
+  return CQG_OK;
+}
+
 cqg_status cqg_get_fusion(cqg_ctx *ctx, int *tier, double *tuned_ms) {
   if (!ctx) return CQG_ERR_BAD_ARG;
   if (tier) *tier = ctx->fused_tier;
@@ -1395,7 +1724,7 @@ cqg_status cqg_get_fusion(cqg_ctx *ctx, int *tier, double *tuned_ms) {
 cqg_status cqg_set_schedule(cqg_ctx *ctx, const int *cta_per_sm, const int *warps_per_cta,
                             const int *quartets_per_warp, const int *warp_form) {
   if (!ctx) return CQG_ERR_BAD_ARG;
-  for (int k = 0; k < 2 * CQG_NQC; ++k) {
+  for (int k = 0; k < CQG_NLIST; ++k) {
     if ((cta_per_sm && (cta_per_sm[k] < 0 || cta_per_sm[k] > 64)) ||
         (warps_per_cta && (warps_per_cta[k] < 0 || warps_per_cta[k] > 4)) ||
         (quartets_per_warp && (quartets_per_warp[k] < 0 || quartets_per_warp[k] > 1024)) ||
@@ -1405,10 +1734,11 @@ cqg_status cqg_set_schedule(cqg_ctx *ctx, const int *cta_per_sm, const int *warp
       return CQG_ERR_BAD_ARG;
     }
   }
-  for (int k = 0; k < 2 * CQG_NQC; ++k) {
+  for (int k = 0; k < CQG_NLIST; ++k) {
     int i, j;
     qclass_split(k % CQG_NQC, i, j);
-    const bool both = is_variant_class(kPairClass[i][0], kPairClass[i][1], kPairClass[j][0], kPairClass[j][1]);
+    const bool both = k < 2 * CQG_NQC &&
+                      is_variant_class(kPairClass[i][0], kPairClass[i][1], kPairClass[j][0], kPairClass[j][1]);
     if (cta_per_sm) ctx->shape_cta[k] = cta_per_sm[k];
     if (warps_per_cta) ctx->shape_wpb[k] = warps_per_cta[k];
     if (quartets_per_warp) ctx->shape_qpw[k] = quartets_per_warp[k];

@@ -20,6 +20,7 @@
 #include "../../include/cqgpu.h"
 #include "eri_common.cuh"
 #include "_gen/eri_classes.cuh"
+#include "_gen/eri_gc_classes.cuh"
 #include "eri_warp.cuh"
 
 #define CQG_MAXL 3
@@ -29,7 +30,11 @@
 #define CQG_NPC ((CQG_MAXL + 1) * (CQG_MAXL + 2) / 2)       // pair classes
 #define CQG_NQC (CQG_NPC * (CQG_NPC + 1) / 2)                // quartet classes
 #define CQG_MAXG 4
-#define CQG_NBUCKET 16
+// Ket buckets of a (molecule, pair class): the primitive-count bucket of the pair's group,
+// and whether the group has one member (kind 0) or more (kind 1):
+// bucket = kind * CQG_NPBUCKET + primitive bucket.
+#define CQG_NPBUCKET 16
+#define CQG_NBUCKET (2 * CQG_NPBUCKET)
 
 static_assert(CQG_NQC <= 55, "class table");
 
@@ -44,6 +49,38 @@ static inline int nfun(int l) { return l > 1 ? 2 * l + 1 : (l + 1) * (l + 2) / 2
 __host__ __device__ constexpr int nfun_c(int l) { return l > 1 ? 2 * l + 1 : (l + 1) * (l + 2) / 2; }
 __host__ __device__ constexpr int ncart_c(int l) { return (l + 1) * (l + 2) / 2; }
 __host__ __device__ constexpr int nherm_c(int n) { return (n + 1) * (n + 2) * (n + 3) / 6; }
+
+// Members a sibling group of a pair class holds at most (larger families are split into
+// groups of this size): s-s pairs 4 (two s shells of one contraction on each centre, or the
+// three distinct pairs of one centre's two), p-s and d-s pairs 2, every other class 1 (not
+// grouped: the classes whose sibling pairs keep one orientation, L_a > L_b, or are
+// symmetric in a and b, s-s).
+__host__ __device__ constexpr int sibling_cap(int la, int lb) {
+  return (la == 0 && lb == 0) ? 4 : ((la == 1 || la == 2) && lb == 0) ? 2 : 1;
+}
+
+// Sibling-group quartet classes (generated sibling form EriClassGC<.., MB, MK>, MB and MK
+// the member caps of the bra and ket pair classes).
+template <int LA, int LB, int LC, int LD>
+struct EriGroup {
+  static constexpr bool ok = false;
+  static constexpr int MB = 1, MK = 1;
+};
+#define CQG_GC_TRAIT(A, B, C, D, MB_, MK_)                                                            \
+  template <>                                                                                       \
+  struct EriGroup<A, B, C, D> {                                                                     \
+    static constexpr bool ok = true;                                                                \
+    static constexpr int MB = MB_, MK = MK_;                                                        \
+    static_assert(MB_ == sibling_cap(A, B) && MK_ == sibling_cap(C, D), "member caps of the class"); \
+  };
+CQG_GC_EACH(CQG_GC_TRAIT)
+#undef CQG_GC_TRAIT
+
+__host__ __device__ constexpr int pair_class_c(int la, int lb) { return la * (la + 1) / 2 + lb; }
+// quartet class index (bra pair class i >= ket pair class j, k = i(i+1)/2 + j)
+__host__ __device__ constexpr int qclass_index(int la, int lb, int lc, int ld) {
+  return pair_class_c(la, lb) * (pair_class_c(la, lb) + 1) / 2 + pair_class_c(lc, ld);
+}
 
 // quartet class k <-> (bra pair class i, ket pair class j), i >= j, k = i(i+1)/2 + j
 static inline void qclass_split(int k, int &i, int &j) {
@@ -71,6 +108,7 @@ struct Mols {
   const int *nbf;                // basis functions of molecule m
   const unsigned char *active;   // molecule m takes part in the call
   const int *molbk;              // [m][ket pair class][bucket + 1]: first pair of each bucket
+  const int *molgbk;             // the same in group index space: first group of each bucket
 };
 struct Pairs {
   const int2 *sh;       // (shell a, shell b), internal orientation L_a >= L_b
@@ -79,6 +117,28 @@ struct Pairs {
   const int *np;        // number of primitive pairs (after primitive screening)
   const int *kk;        // nprim(a) * nprim(b) of the contracted shells (model count)
   const PrimPair *prim;
+  // Sibling groups: pairs whose shells have the same centres, angular momenta and
+  // exponents (segmented copies of one general contraction) and differ only in their
+  // contraction coefficients.  The members of a group are consecutive pairs, led by the
+  // first.  Group g (group index space, in pair order) is led by pair glead[g]; gQ[g] is
+  // the largest Q of its members and Qc[i] that of pair i's group (non-increasing within a
+  // primitive bucket, so it serves the coarse range searches).
+  const double *Qc;
+  const int *glead;
+  const double *gQ;
+  // Per pair (meaningful for leaders): gsz members (0 for the other members), and the
+  // group's unit-coefficient primitive pairs gprim[gpoff .. gpoff + gnp) (the union of the
+  // members' screened primitive pairs) with the members' coefficient products
+  // gw[gwoff + m * gnp + i], m < the member cap of the pair class (zero rows past gsz).
+  const int *gsz;
+  const int *gpoff;
+  const int *gnp;
+  const int *gwoff;
+  const PrimPair *gprim;
+  const double *gw;
+  // Member masks of the sibling-group list entries (bit 4 i + j: bra member i with ket
+  // member j), parallel to the quartet list.
+  const unsigned short *qmask;
 };
 struct DigestGroups {
   const double *X[CQG_MAXG];
@@ -201,6 +261,9 @@ struct BlockTable {
   int ket_n[CQG_NQC];          // number of ket pairs of the block's ket class
   int diag[CQG_NQC];           // bra class == ket class
   int ket_class[CQG_NQC];      // pair class of the ket
+  int grouped[CQG_NQC];        // tasks are bra sibling groups
+  int gbra_beg[CQG_NQC];       // first bra group (group index) of a grouped block
+  int min_members[CQG_NQC];    // grouped: member quartets a sibling entry holds at least
 };
 
 __device__ __forceinline__ int find_block(const BlockTable &bt, int task) {
@@ -248,10 +311,45 @@ static __global__ void k_pairnorm(const int2 *__restrict__ sh, int npairs, Mols 
   Mpair[i] = M[mols.Moff[mol] + (ab.x - shoff) + (size_t)(ab.y - shoff) * nsh];
 }
 
+// Per-block screening tallies in blkacc[kBlkAcc * blk + ...]: model primitive quartets
+// (sum of Ka Kb Kc Kd) and executed primitive quartets of the FP64 and FP32 lists, then the
+// number of contracted quartets of each (a sibling-group entry holds several).
+constexpr int kBlkAcc = 6;
+
+// The quartet list is laid out by virtual task v = part * ntask + task, part 0 / 1 = the
+// FP64 / FP32 pair entries (one quartet each), part 2 / 3 = the FP64 / FP32 sibling-group
+// entries; work list vb = part * CQG_NQC + class is the range of one part of one class.
+constexpr int kListParts = 4;
+#define CQG_NLIST (kListParts * CQG_NQC)
+constexpr int kRangeThreads = 256;   // k_block_ranges: one thread per work list
+static_assert(CQG_NLIST <= kRangeThreads, "k_block_ranges needs a thread per work list");
+
+// exclusive prefix sum over the warp's lanes and the warp's total
+__device__ __forceinline__ unsigned warp_excl_scan(unsigned x, unsigned &total) {
+  const int lane = threadIdx.x & 31;
+  unsigned v = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += y;
+  }
+  total = __shfl_sync(0xffffffffu, v, 31);
+  return v - x;
+}
+
 // Count (FILL=false) or write (FILL=true) the passing quartets of each task.  One warp
-// per task; ket pairs scanned in ascending order, survivors compacted with a ballot so
-// the list is deterministic.  Quartets whose bound is below `cut32` go to the FP32 list
-// (counts cnt[ntask + task], offsets off[ntask + task]); the rest to the FP64 list.
+// per task; ket pairs scanned in ascending order, survivors compacted in lane order so the
+// list is deterministic.  Quartets whose bound is below `cut32` go to the FP32 parts; the
+// rest to the FP64 parts.  Counts cnt[v], offsets off[v] per virtual task v.
+//
+// In a grouped block a task is one bra sibling group and each lane takes one ket group:
+// every member quartet (bra member i, ket member j) gets the exact test above.  A pair of
+// groups with at least bt.min_members[blk] member quartets becomes one sibling entry (bra
+// leader, ket leader) per precision, with the mask of its members that passed at that
+// precision; the members of a smaller pair of groups become pair entries of their own.  So
+// the contracted quartets, their count and their precision are those of the pair-level
+// lists.  In a diagonal block (bra class = ket class) ket group <= bra group, and within one
+// group ket member <= bra member, so every unordered pair of pairs is taken once.
 template <bool FILL>
 __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pairs P, const double *__restrict__ M,
                                                   const double *__restrict__ MT, const double *__restrict__ Mpair,
@@ -259,66 +357,160 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
                                                   const double *__restrict__ Mmax, double thresh,
                                                   double cut32, long long *__restrict__ cnt,
                                                   const long long *__restrict__ off, uint2 *__restrict__ qlist,
+                                                  unsigned short *__restrict__ qmask,
                                                   unsigned long long *__restrict__ blkacc, long long vt0,
                                                   long long vt1, long long obase, long long cap) {
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (warp >= ntask) return;
-  // fill pass: only the FP64 (virtual task warp) and FP32 (ntask + warp) parts inside the chunk
-  const bool do64 = !FILL || (warp >= vt0 && warp < vt1);
-  const bool do32 = !FILL || (ntask + warp >= vt0 && ntask + warp < vt1);
-  if (FILL && !do64 && !do32) return;
-  int blk = find_block(bt, warp);
-  int bra = bt.bra_beg[blk] + (warp - bt.task_beg[blk]);
-  double qb = P.Q[bra];
+  // fill pass: only the parts (virtual tasks part * ntask + warp) inside the chunk
+  bool dop[kListParts];
+  bool any = false;
+#pragma unroll
+  for (int p = 0; p < kListParts; ++p) {
+    const long long v = (long long)p * ntask + warp;
+    dop[p] = !FILL || (v >= vt0 && v < vt1);
+    any = any || dop[p];
+  }
+  if (FILL && !any) return;
+  const int blk = find_block(bt, warp);
+  const bool grouped = bt.grouped[blk] != 0;
+  // Tasks take the class's bra pairs (groups) from the last: the pairs are ordered by
+  // primitive-count bucket, so the list starts with the heaviest quartets and the work
+  // queues hand out the light ones at the end of a launch.
+  const int t = bt.task_beg[blk + 1] - 1 - warp;
+  const int gbra = grouped ? bt.gbra_beg[blk] + t : -1;
+  const int bra = grouped ? P.glead[gbra] : bt.bra_beg[blk] + t;
+  const int mb = grouped ? P.gsz[bra] : 1;
+  const int min_members = bt.min_members[blk];
+  const double qb = grouped ? P.gQ[gbra] : P.Q[bra];
   double mm = *Mmax;
   double cut = (qb * mm > 0.0) ? thresh / (qb * mm) * (1.0 - 1e-12) : 0.0;
   int2 ab = P.sh[bra];
   const int mol = shmol[ab.x];
   const int nsh = mols.nsh[mol], shoff = mols.shoff[mol];
   const double *Mm = M + mols.Moff[mol];
-  const double *col1 = MT + mols.Moff[mol] + (size_t)(ab.x - shoff) * nsh;
-  const double *col2 = MT + mols.Moff[mol] + (size_t)(ab.y - shoff) * nsh;
+  const double *MTm = MT + mols.Moff[mol];
+  const double *col1 = MTm + (size_t)(ab.x - shoff) * nsh;
+  const double *col2 = MTm + (size_t)(ab.y - shoff) * nsh;
   const double m12 = Mm[(ab.x - shoff) + (size_t)(ab.y - shoff) * nsh];
-  const int *bkt = mols.molbk + ((size_t)mol * CQG_NPC + bt.ket_class[blk]) * (CQG_NBUCKET + 1);
-  const long long base64 = FILL ? off[warp] - obase : 0, base32 = FILL ? off[ntask + warp] - obase : 0;
-  long long c64 = 0, c32 = 0;
-  unsigned long long km64 = 0, ke64 = 0, km32 = 0, ke32 = 0;
+  const int *bkt = (grouped ? mols.molgbk : mols.molbk) + ((size_t)mol * CQG_NPC + bt.ket_class[blk]) * (CQG_NBUCKET + 1);
+  const double *Qs = grouped ? P.gQ : P.Qc;   // non-increasing within each bucket
+  long long base[kListParts], cpart[kListParts];
+#pragma unroll
+  for (int p = 0; p < kListParts; ++p) {
+    base[p] = FILL ? off[(long long)p * ntask + warp] - obase : 0;
+    cpart[p] = 0;
+  }
+  unsigned long long km64 = 0, ke64 = 0, km32 = 0, ke32 = 0, nq64 = 0, nq32 = 0;
   if (qb * mm > 0.0 && mols.active[mol]) {
     for (int bk = 0; bk < CQG_NBUCKET; ++bk) {
       const int kb = bkt[bk], ke = bkt[bk + 1];
       if (ke <= kb) continue;
-      int kend = kb + coarse_range(P.Q, kb, ke - kb, cut);
-      if (bt.diag[blk]) kend = min(kend, bra + 1);   // unique pairs of pairs: ket <= bra
+      int kend = kb + coarse_range(Qs, kb, ke - kb, cut);
+      if (bt.diag[blk]) kend = min(kend, (grouped ? gbra : bra) + 1);   // unique pairs of pairs
       for (int k0 = kb; k0 < kend; k0 += 32) {
-        int ket = k0 + lane;
-        bool pass = false, lo = false;
-        if (ket < kend) {
-          const double bnd = quartet_bound(col1, col2, m12, Mpair[ket], shoff, P.sh[ket], qb, P.Q[ket]);
-          pass = bnd >= thresh;
-          lo = pass && bnd < cut32;
+        const int kx = k0 + lane;   // ket pair, or ket group in a grouped block
+        int ket = 0;
+        unsigned m64 = 0, m32 = 0;   // member masks (bit 4 i + j); pair blocks: bit 0
+        bool sib = false;            // grouped: the pair of groups is one sibling entry
+        if (kx < kend) {
+          if (!grouped) {
+            ket = kx;
+            const double bnd = quartet_bound(col1, col2, m12, Mpair[ket], shoff, P.sh[ket], qb, P.Q[ket]);
+            if (bnd >= thresh) {
+              if (bnd < cut32) m32 = 1u; else m64 = 1u;
+            }
+            if (!FILL && m64) {
+              km64 += (unsigned long long)P.kk[ket] * (unsigned long long)P.kk[bra];
+              ke64 += (unsigned long long)P.np[ket] * (unsigned long long)P.np[bra];
+            }
+            if (!FILL && m32) {
+              km32 += (unsigned long long)P.kk[ket] * (unsigned long long)P.kk[bra];
+              ke32 += (unsigned long long)P.np[ket] * (unsigned long long)P.np[bra];
+            }
+          } else {
+            ket = P.glead[kx];
+            const int mk = P.gsz[ket];
+            const bool same = bt.diag[blk] && kx == gbra;
+            sib = mb * mk > 1 && (same ? mb * (mb + 1) / 2 : mb * mk) >= min_members;
+            for (int i = 0; i < mb; ++i) {
+              const int bi = bra + i;
+              const int2 abi = P.sh[bi];
+              const double *c1 = MTm + (size_t)(abi.x - shoff) * nsh;
+              const double *c2 = MTm + (size_t)(abi.y - shoff) * nsh;
+              const double mi = Mpair[bi], qi = P.Q[bi];
+              const int jmax = same ? min(mk, i + 1) : mk;
+              for (int j = 0; j < jmax; ++j) {
+                const int kj = ket + j;
+                const double bnd = quartet_bound(c1, c2, mi, Mpair[kj], shoff, P.sh[kj], qi, P.Q[kj]);
+                if (bnd < thresh) continue;
+                const unsigned bit = 1u << (4 * i + j);
+                const unsigned long long kq = (unsigned long long)P.kk[bi] * (unsigned long long)P.kk[kj];
+                // executed primitive quartets of a member quartet evaluated on its own
+                const unsigned long long eq =
+                    sib ? 0ull : (unsigned long long)P.np[bi] * (unsigned long long)P.np[kj];
+                if (bnd < cut32) {
+                  m32 |= bit;
+                  if (!FILL) {
+                    km32 += kq;
+                    ke32 += eq;
+                  }
+                } else {
+                  m64 |= bit;
+                  if (!FILL) {
+                    km64 += kq;
+                    ke64 += eq;
+                  }
+                }
+              }
+            }
+            if (!FILL && sib) {   // a sibling entry evaluates the groups' shared primitive pairs once
+              const unsigned long long gq = (unsigned long long)P.gnp[bra] * (unsigned long long)P.gnp[ket];
+              if (m64) ke64 += gq;
+              if (m32) ke32 += gq;
+            }
+          }
         }
-        const bool hi = pass && !lo;
-        unsigned b64 = __ballot_sync(0xffffffffu, hi), b32 = __ballot_sync(0xffffffffu, lo);
-        const unsigned below = (1u << lane) - 1u;
-        if (FILL && hi && do64) {
-          const long long pos = base64 + c64 + __popc(b64 & below);
-          if (pos < cap) qlist[pos] = make_uint2((unsigned)bra, (unsigned)ket);
+        if (!FILL) {
+          nq64 += (unsigned long long)__popc(m64);
+          nq32 += (unsigned long long)__popc(m32);
         }
-        if (FILL && lo && do32) {
-          const long long pos = base32 + c32 + __popc(b32 & below);
-          if (pos < cap) qlist[pos] = make_uint2((unsigned)bra, (unsigned)ket);
+        // entries of this lane per part: pair entries one per member quartet, sibling entries one per mask
+        unsigned n[kListParts];
+        n[0] = sib ? 0u : (unsigned)__popc(m64);
+        n[1] = sib ? 0u : (unsigned)__popc(m32);
+        n[2] = (sib && m64) ? 1u : 0u;
+        n[3] = (sib && m32) ? 1u : 0u;
+#pragma unroll
+        for (int p = 0; p < kListParts; ++p) {
+          unsigned total, before;
+          if (grouped && p < 2) {   // several pair entries per lane
+            before = warp_excl_scan(n[p], total);
+          } else {                  // at most one entry per lane
+            const unsigned b = __ballot_sync(0xffffffffu, n[p] != 0);
+            before = __popc(b & ((1u << lane) - 1u));
+            total = __popc(b);
+          }
+          if (FILL && dop[p] && n[p]) {
+            long long pos = base[p] + cpart[p] + before;
+            if (p >= 2) {
+              if (pos < cap) {
+                qlist[pos] = make_uint2((unsigned)bra, (unsigned)ket);
+                qmask[pos] = (unsigned short)(p == 2 ? m64 : m32);
+              }
+            } else {
+              unsigned m = p == 0 ? m64 : m32;
+              while (m) {   // member quartets in bit order
+                const int bit = __ffs(m) - 1;
+                m &= m - 1;
+                if (pos < cap) qlist[pos] = make_uint2((unsigned)(bra + (bit >> 2)), (unsigned)(ket + (bit & 3)));
+                ++pos;
+              }
+            }
+          }
+          cpart[p] += total;
         }
-        if (!FILL && hi) {
-          km64 += (unsigned long long)P.kk[ket];
-          ke64 += (unsigned long long)P.np[ket];
-        }
-        if (!FILL && lo) {
-          km32 += (unsigned long long)P.kk[ket];
-          ke32 += (unsigned long long)P.np[ket];
-        }
-        c64 += __popc(b64);
-        c32 += __popc(b32);
       }
     }
   }
@@ -328,32 +520,38 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
       ke64 += __shfl_xor_sync(0xffffffffu, ke64, o);
       km32 += __shfl_xor_sync(0xffffffffu, km32, o);
       ke32 += __shfl_xor_sync(0xffffffffu, ke32, o);
+      nq64 += __shfl_xor_sync(0xffffffffu, nq64, o);
+      nq32 += __shfl_xor_sync(0xffffffffu, nq32, o);
     }
     if (lane == 0) {
-      cnt[warp] = c64;
-      cnt[ntask + warp] = c32;
-      if (c64) {
-        atomicAdd(blkacc + 4 * blk + 0, km64 * (unsigned long long)P.kk[bra]);
-        atomicAdd(blkacc + 4 * blk + 1, ke64 * (unsigned long long)P.np[bra]);
+#pragma unroll
+      for (int p = 0; p < kListParts; ++p) cnt[(long long)p * ntask + warp] = cpart[p];
+      unsigned long long *acc = blkacc + kBlkAcc * blk;
+      if (nq64) {
+        atomicAdd(acc + 0, km64);
+        atomicAdd(acc + 1, ke64);
+        atomicAdd(acc + 4, nq64);
       }
-      if (c32) {
-        atomicAdd(blkacc + 4 * blk + 2, km32 * (unsigned long long)P.kk[bra]);
-        atomicAdd(blkacc + 4 * blk + 3, ke32 * (unsigned long long)P.np[bra]);
+      if (nq32) {
+        atomicAdd(acc + 2, km32);
+        atomicAdd(acc + 3, ke32);
+        atomicAdd(acc + 5, nq32);
       }
     }
   }
 }
 
-// Ranges [beg, end) of the quartet list per (precision, class block) from the per-task
-// counts and offsets; virtual block b = prec * nblk + block, prec 0 = FP64, 1 = FP32.
+// Ranges [beg, end) of the quartet list per work list vb = part * nblk + block from the
+// per-task counts and offsets (virtual task part * ntask + task).
 static __global__ void k_block_ranges(BlockTable bt, int ntask, const long long *__restrict__ cnt,
                                const long long *__restrict__ off, long long *__restrict__ range, long long cap,
                                int *__restrict__ flags) {
   int vb = threadIdx.x;
-  if (vb == 0 && ntask > 0 && off[2 * ntask - 1] + cnt[2 * ntask - 1] > cap) flags[2] = 1;   // list overflow
-  if (vb >= 2 * bt.nblk) return;
-  const int prec = vb / bt.nblk, b = vb % bt.nblk;
-  const int t0 = prec * ntask + bt.task_beg[b], t1 = prec * ntask + bt.task_beg[b + 1];
+  const long long nv = (long long)kListParts * ntask;
+  if (vb == 0 && ntask > 0 && off[nv - 1] + cnt[nv - 1] > cap) flags[2] = 1;   // list overflow
+  if (vb >= kListParts * bt.nblk) return;
+  const int part = vb / bt.nblk, b = vb % bt.nblk;
+  const long long t0 = (long long)part * ntask + bt.task_beg[b], t1 = (long long)part * ntask + bt.task_beg[b + 1];
   long long beg = 0, end = 0;
   if (t1 > t0) {
     beg = off[t0];
@@ -539,13 +737,11 @@ __global__ void __launch_bounds__(kEriThreads) k_eri_jk(const uint2 *__restrict_
   }
 }
 
+// One list entry (pair quartet) per lane with the class's per-thread code and its digest.
 template <int LA, int LB, int LC, int LD, typename T>
-__device__ __forceinline__ void eri_jk_one(const uint2 *__restrict__ ql, long long i, long long wfirst, long long end,
-                                           const Pairs &P, const Shells &S, const double *boys,
-                                           const DigestGroups &dg) {
-  const bool valid = i < end;
+__device__ __forceinline__ void eri_jk_plain(const uint2 e, const bool valid, const Pairs &P, const Shells &S,
+                                             const double *boys, const DigestGroups &dg) {
   constexpr int NA = nfun_c(LA), NB = nfun_c(LB), NC = nfun_c(LC), ND = nfun_c(LD);
-  const uint2 e = ql[valid ? i : wfirst];
   const int2 ab = P.sh[e.x], cd = P.sh[e.y];
   double v[NA * NB * NC * ND];
   if (valid) {
@@ -568,6 +764,93 @@ __device__ __forceinline__ void eri_jk_one(const uint2 *__restrict__ ql, long lo
   const bool uniform = __all_sync(0xffffffffu, e.x == bra0);
   const double deg = (ab.x == ab.y ? 1.0 : 2.0) * (cd.x == cd.y ? 1.0 : 2.0) * (e.x == e.y ? 1.0 : 2.0);
   digest<NA, NB, NC, ND>(v, deg, S.bf[ab.x], S.bf[ab.y], S.bf[cd.x], S.bf[cd.y], dg, valid, uniform, S.mol[ab.x]);
+}
+
+// One sibling-group entry per lane: the generated sibling form evaluates the MB x MK member
+// quartets (bra members leader e.x + i, ket members e.y + j) from one pass over the groups'
+// primitive pairs, then each member quartet of the entry's mask is digested as a quartet of
+// its own.
+template <int LA, int LB, int LC, int LD, typename T>
+__device__ __forceinline__ void eri_jk_group(const uint2 e, const bool valid, const unsigned mask, const Pairs &P,
+                                             const Shells &S, const double *boys, const DigestGroups &dg) {
+  constexpr int NA = nfun_c(LA), NB = nfun_c(LB), NC = nfun_c(LC), ND = nfun_c(LD);
+  constexpr int NQ = NA * NB * NC * ND;
+  constexpr int MB = EriGroup<LA, LB, LC, LD>::MB, MK = EriGroup<LA, LB, LC, LD>::MK;
+  const int mb = P.gsz[e.x], mk = P.gsz[e.y];
+  double v[MB * MK * NQ];
+  if (valid) {
+    const int2 ab = P.sh[e.x], cd = P.sh[e.y];
+    const double3 A = S.center[ab.x], B = S.center[ab.y], C = S.center[cd.x], D = S.center[cd.y];
+    const PrimPair *bp = P.gprim + P.gpoff[e.x], *kp = P.gprim + P.gpoff[e.y];
+    const double *bw = P.gw + P.gwoff[e.x], *kw = P.gw + P.gwoff[e.y];
+    if constexpr (sizeof(T) == sizeof(double)) {
+      EriClassGC<LA, LB, LC, LD, MB, MK>::template run<double>(bp, bw, P.gnp[e.x], kp, kw, P.gnp[e.y], A, B, C, D,
+                                                               boys, v);
+    } else {
+      T vt[MB * MK * NQ];
+      EriClassGC<LA, LB, LC, LD, MB, MK>::template run<T>(bp, bw, P.gnp[e.x], kp, kw, P.gnp[e.y], A, B, C, D, boys,
+                                                          vt);
+#pragma unroll
+      for (int k = 0; k < MB * MK * NQ; ++k) v[k] = (double)vt[k];
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < MB * MK * NQ; ++k) v[k] = 0.0;
+  }
+  const unsigned bra0 = __shfl_sync(0xffffffffu, e.x, 0);
+  const bool uniform = __all_sync(0xffffffffu, e.x == bra0);
+#pragma unroll
+  for (int i = 0; i < MB; ++i) {
+#pragma unroll
+    for (int j = 0; j < MK; ++j) {
+      const bool mv = valid && ((mask >> (4 * i + j)) & 1u);
+      if (!__any_sync(0xffffffffu, mv)) continue;
+      // members past the group's size are never in the mask; their lanes address the leader
+      const int pa = i < mb ? (int)e.x + i : (int)e.x;
+      const int pc = j < mk ? (int)e.y + j : (int)e.y;
+      const int2 ab = P.sh[pa], cd = P.sh[pc];
+      const double deg = (ab.x == ab.y ? 1.0 : 2.0) * (cd.x == cd.y ? 1.0 : 2.0) * (pa == pc ? 1.0 : 2.0);
+      digest<NA, NB, NC, ND>(v + (i * MK + j) * NQ, deg, S.bf[ab.x], S.bf[ab.y], S.bf[cd.x], S.bf[cd.y], dg, mv,
+                             uniform, S.mol[ab.x]);
+    }
+  }
+}
+
+template <int LA, int LB, int LC, int LD, typename T>
+__device__ __forceinline__ void eri_jk_one(const uint2 *__restrict__ ql, long long i, long long wfirst, long long end,
+                                           const Pairs &P, const Shells &S, const double *boys,
+                                           const DigestGroups &dg) {
+  const bool valid = i < end;
+  const uint2 e = ql[valid ? i : wfirst];
+  eri_jk_plain<LA, LB, LC, LD, T>(e, valid, P, S, boys, dg);
+}
+
+// Sibling-group list of class (LA LB|LC LD): the work queue and persistent grid of
+// k_eri_jk, one entry (bra group, ket group, member mask) per thread.
+template <int LA, int LB, int LC, int LD, typename T>
+__global__ void __launch_bounds__(kEriThreads) k_eri_gc(const uint2 *__restrict__ ql, const long long *__restrict__ range,
+                                                int blk, Pairs P, Shells S, const double *__restrict__ boys_g,
+                                                DigestGroups dg, unsigned long long *__restrict__ qhead, int chunk) {
+  __shared__ __align__(16) double boys[BOYS_NT * BOYS_SROW];
+  stage_boys<LA + LB + LC + LD>(boys_g, boys);
+  __syncthreads();
+  const long long beg = range[2 * blk], end = range[2 * blk + 1];
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned long long c0 = 0;
+    if (lane == 0) c0 = atomicAdd(qhead + blk, (unsigned long long)chunk);
+    c0 = __shfl_sync(0xffffffffu, c0, 0);
+    const long long cfirst = beg + (long long)c0;
+    if (cfirst >= end) return;   // the whole list is claimed
+    const long long cend = min(cfirst + (long long)chunk, end);
+    for (long long wfirst = cfirst; wfirst < cend; wfirst += 32) {
+      const long long i = wfirst + lane;
+      const bool valid = i < cend;
+      const uint2 e = ql[valid ? i : wfirst];
+      const unsigned mask = valid ? (unsigned)P.qmask[i] : 0u;
+      eri_jk_group<LA, LB, LC, LD, T>(e, valid, mask, P, S, boys, dg);
+    }
+  }
 }
 
 // ------------------------------------------------------------- warp-mode classes ---
@@ -1159,18 +1442,18 @@ struct cqg_ctx {
   int nsm = 148;                       // multiprocessors of the device
   // launch shapes per (precision, class) work list: persistent CTAs per SM and, for the
   // warp-cooperative classes, warps per CTA (0 = default); set by the autotuner
-  int shape_cta[2 * CQG_NQC] = {0};
-  int shape_wpb[2 * CQG_NQC] = {0};
+  int shape_cta[CQG_NLIST] = {0};
+  int shape_wpb[CQG_NLIST] = {0};
   // quartets a warp claims from the list's work queue at a time, in units of 32 for the
   // per-thread classes (0 = default)
-  int shape_qpw[2 * CQG_NQC] = {0};
+  int shape_qpw[CQG_NLIST] = {0};
   // kernel form of a list whose class has both: 0 = per-thread (default), 1 = warp-cooperative
-  int shape_var[2 * CQG_NQC] = {0};
+  int shape_var[CQG_NLIST] = {0};
   // 0: one launch per class list; 1 or 2: the lists of that tier's classes go through one
   // class-fused persistent kernel (eri_fused.cu); set by the autotuner or cqg_set_fusion
   int fused_tier = 0;
   double fusion_ms[3] = {0.0, 0.0, 0.0};   // autotuner's times of the three forms (ms)
-  DevBuf<unsigned long long> d_qhead;  // work-queue head counter of every (precision, class) list
+  DevBuf<unsigned long long> d_qhead;  // work-queue head counter of every work list, then the fused one
   int autotune_pending = 0;
   long long graph_capacity = 0;        // > 0: sync-free contraction for CUDA-graph capture
   bool class_possible[CQG_NQC] = {false};
@@ -1216,9 +1499,24 @@ struct cqg_ctx {
   DevBuf<unsigned char> d_scan_tmp;
   DevBuf<uint2> d_qlist;
   DevBuf<double> d_G, d_X, d_AX, d_Gscratch;
-  BlockTable bt;
+  BlockTable bt;                      // the active table (bt_pair or bt_group)
   int ntask = 0;
-  cudaEvent_t ev[4 + 2 * 55 + 2];
+  BlockTable bt_pair, bt_group;       // pair tasks everywhere / bra-group tasks for the sibling classes
+  int ntask_pair = 0, ntask_group = 0;
+  // sibling groups (Pairs): on = the sibling classes get sibling-entry lists
+  int siblings = 0;
+  // grouped classes: smallest number of member quartets of a pair of groups that makes a
+  // sibling entry (smaller ones become pair entries); set from the sibling form's size
+  int sibling_min[CQG_NQC] = {0};
+  std::vector<int> pair_gsz, glead;
+  std::vector<double> pair_Qc, gQ;
+  int gc_beg[CQG_NPC + 1] = {0};      // first group of each pair class
+  long long group_prim_pairs = 0;
+  DevBuf<int> d_molgbk, d_gsz, d_gpoff, d_gnp, d_gwoff, d_glead;
+  DevBuf<double> d_pair_Qc, d_gQ, d_gw;
+  DevBuf<PrimPair> d_gprim;
+  DevBuf<unsigned short> d_qmask;     // member masks, parallel to d_qlist
+  cudaEvent_t ev[4 + 2 * CQG_NQC + 2];
   bool events = false;
   cqg_stats stats;
   double *oe_table = nullptr;   // device address of the fixed charge table (cqg_one_e_noalloc)
@@ -1296,6 +1594,16 @@ static inline Pairs make_pairs(cqg_ctx *ctx) {
   P.np = ctx->d_pair_np.p;
   P.kk = ctx->d_pair_kk.p;
   P.prim = ctx->d_prim.p;
+  P.Qc = ctx->d_pair_Qc.p;
+  P.glead = ctx->d_glead.p;
+  P.gQ = ctx->d_gQ.p;
+  P.gsz = ctx->d_gsz.p;
+  P.gpoff = ctx->d_gpoff.p;
+  P.gnp = ctx->d_gnp.p;
+  P.gwoff = ctx->d_gwoff.p;
+  P.gprim = ctx->d_gprim.p;
+  P.gw = ctx->d_gw.p;
+  P.qmask = ctx->d_qmask.p;
   return P;
 }
 static inline Shells make_shells(cqg_ctx *ctx) {
@@ -1315,10 +1623,25 @@ static inline Mols make_mols(cqg_ctx *ctx) {
   M.nbf = ctx->d_mnbf.p;
   M.active = ctx->d_active.p;
   M.molbk = ctx->d_molbk.p;
+  M.molgbk = ctx->d_molgbk.p;
   return M;
 }
 
 typedef cudaError_t (*eri_launcher)(cqg_ctx *, int blk, long long n, cudaStream_t st, const DigestGroups &dg);
+
+// One launch of the sibling-group kernel of class (LA LB|LC LD) over list blk.
+template <int LA, int LB, int LC, int LD, typename T>
+static cudaError_t launch_gc(cqg_ctx *ctx, int blk, long long n, cudaStream_t st, const DigestGroups &dg) {
+  if (n == 0) return cudaSuccess;   // n < 0: count unknown on the host (graph mode)
+  const int cta = ctx->shape_cta[blk] > 0 ? ctx->shape_cta[blk] : 4;
+  const long long cap = (long long)ctx->nsm * cta;
+  const long long nb = n > 0 ? std::min<long long>((n + kEriThreads - 1) / kEriThreads, cap) : cap;
+  const int chunk = 32 * (ctx->shape_qpw[blk] > 0 ? ctx->shape_qpw[blk] : 1);
+  k_eri_gc<LA, LB, LC, LD, T><<<(unsigned)nb, kEriThreads, 0, st>>>(ctx->d_qlist.p, ctx->d_range.p, blk,
+                                                                   make_pairs(ctx), make_shells(ctx), ctx->d_boys.p,
+                                                                   dg, ctx->d_qhead.p, chunk);
+  return cudaGetLastError();
+}
 
 // Class-fused schedule (eri_fused.cu): whether class (la lb|lc ld) belongs to the fused
 // kernel of `tier` (1: (ss|ss) and (ps|ss), 2: every per-thread class up to (dd|dd)), and one

@@ -163,17 +163,17 @@ bool cqg_fused_member(int tier, int la, int lb, int lc, int ld) {
 }
 
 // One launch of the fused kernel of `tier` over the current list ranges (d_range); the
-// head counter d_qhead[2 * CQG_NQC] is zeroed on the stream first.
+// head counter d_qhead[CQG_NLIST] is zeroed on the stream first.
 cudaError_t cqg_launch_fused(cqg_ctx *ctx, int tier, cudaStream_t st, const DigestGroups &dg) {
-  cudaError_t e = cudaMemsetAsync(ctx->d_qhead.p + 2 * CQG_NQC, 0, sizeof(unsigned long long), st);
+  cudaError_t e = cudaMemsetAsync(ctx->d_qhead.p + CQG_NLIST, 0, sizeof(unsigned long long), st);
   if (e != cudaSuccess) return e;
   const int per_sm = tier == 1 ? 4 : 2;
   const unsigned blocks = (unsigned)(ctx->nsm * per_sm);
   if (tier == 1)
     k_eri_fused<1><<<blocks, kEriThreads, 0, st>>>(ctx->d_qlist.p, ctx->d_range.p, make_pairs(ctx), make_shells(ctx),
-                                                   ctx->d_boys.p, dg, ctx->d_qhead.p + 2 * CQG_NQC);
+                                                   ctx->d_boys.p, dg, ctx->d_qhead.p + CQG_NLIST);
   else
     k_eri_fused<2><<<blocks, kEriThreads, 0, st>>>(ctx->d_qlist.p, ctx->d_range.p, make_pairs(ctx), make_shells(ctx),
-                                                   ctx->d_boys.p, dg, ctx->d_qhead.p + 2 * CQG_NQC);
+                                                   ctx->d_boys.p, dg, ctx->d_qhead.p + CQG_NLIST);
   return cudaGetLastError();
 }

@@ -28,6 +28,7 @@ from :file:`boys.cuh` in FP64 regardless of ``T``; everything after them runs in
 Run:  python gen_eri.py <out.cuh> [maxl]
 """
 import itertools
+import os
 import sys
 from math import comb, sqrt, floor
 
@@ -489,9 +490,20 @@ BRA_TILE = {(0, 0, 0, 0): 4}
 KET_TILE = {}
 
 
+# Sibling-group classes of the engine (la, lb, lc, ld, mb, mk): their lists hold entries of
+# one bra and one ket group of sibling pairs (same centres, angular momenta and exponents),
+# evaluated from one set of primitive integrals with mb bra and mk ket member weights.  mb
+# and mk are the member caps of the bra and ket pair classes (s-s pairs 4, p-s and d-s 2,
+# p-p 1; csrc/engine_impl.cuh, sibling_cap); the classes are the per-thread ones whose
+# sibling form stays within the register file.
+GROUP_SPECS = [(0, 0, 0, 0, 4, 4), (1, 0, 0, 0, 2, 4), (1, 0, 1, 0, 2, 2), (1, 1, 0, 0, 1, 4),
+               (2, 0, 0, 0, 2, 4)]
+
+
 def members_header(specs):
     """Header text with the sibling-member variants for `specs` = [(la, lb, lc, ld, mb, mk)],
-    each behind EriClassGC<la, lb, lc, ld, mb, mk>::run, and the list macro CQG_GC_LIST."""
+    each behind EriClassGC<la, lb, lc, ld, mb, mk>::run, the list macro CQG_GC_LIST and the
+    per-spec macro CQG_GC_EACH."""
     parts = ["// GENERATED by gen_eri.py (sibling-member variants) -- do not edit.",
              "#pragma once",
              "#include \"../eri_common.cuh\"",
@@ -510,6 +522,7 @@ def members_header(specs):
         parts.append("};")
         parts.append("")
     parts.append("#define CQG_GC_LIST(X) {" + ", ".join("X(%d, %d, %d, %d, %d, %d)" % q for q in specs) + "}")
+    parts.append("#define CQG_GC_EACH(X) " + " ".join("X(%d, %d, %d, %d, %d, %d)" % q for q in specs))
     return "\n".join(parts) + "\n"
 
 
@@ -544,6 +557,8 @@ def main(path, maxl=2):
     parts.append("")
     with open(path, "w") as f:
         f.write("\n".join(parts))
+    with open(os.path.join(os.path.dirname(os.path.abspath(path)), "eri_gc_classes.cuh"), "w") as f:
+        f.write(members_header([q for q in GROUP_SPECS if max(q[:4]) <= maxl]))
 
 
 if __name__ == "__main__":

@@ -65,6 +65,9 @@ typedef struct {
   double class_ms[55];             /* device time per class kernel (ms), if timing on */
   double ms_fused;                 /* device time of the class-fused kernel (ms), if timing on */
   int fused_tier;                  /* 0: per-class launches; 1, 2: class-fused tier used */
+  long long list_entries;          /* quartet-list entries (a sibling-group entry holds up to 16
+                                      quartets; without siblings one entry per quartet) */
+  long long sibling_classes;       /* bit k set: class k's lists held sibling-group entries */
 } cqg_stats;
 
 /* Library / context lifetime. */
@@ -192,7 +195,8 @@ cqg_status cqg_graph_status(cqg_ctx *ctx, long long *quartets, int *overflow, in
  * shape of each class work list (persistent CTAs per SM; warps per CTA for the
  * warp-cooperative classes; quartets claimed per warp from the list's work queue) and keeps
  * the fastest for later calls.  The shapes are read
- * back with cqg_get_launch_shapes (2 x 55 entries: FP64 lists then FP32 lists; 0 = default). */
+ * back with cqg_get_launch_shapes (cqg_schedule_lists() entries: FP64 lists then FP32 lists;
+ * 0 = default). */
 cqg_status cqg_autotune_next(cqg_ctx *ctx);
 /* Set which molecules of a batch take part in the following contractions (NULL: all);
  * a synchronous copy, to be called outside any captured region. */
@@ -223,15 +227,41 @@ cqg_status cqg_get_fusion(cqg_ctx *ctx, int *tier, double *tuned_ms);
 cqg_status cqg_set_schedule(cqg_ctx *ctx, const int *cta_per_sm, const int *warps_per_cta,
                             const int *quartets_per_warp, const int *warp_form);
 
+/* Sibling groups (off by default).  Shell pairs whose shells share centres, angular momenta
+ * and primitive exponents -- the segmented shells of one general contraction, such as the
+ * 1s and 2s shells of cc-pVXZ oxygen -- differ only in their contraction coefficients.  With
+ * siblings on, the classes (ss|ss), (ps|ss), (ps|ps), (pp|ss) and (ds|ss) get a second pair
+ * of work lists of sibling entries: a bra and a ket group of such pairs with a mask of the
+ * member quartets that pass the screen, evaluated from one pass over the groups' shared
+ * primitive pairs.  The quartets evaluated, their count, their precision and their digest are
+ * those of the pair-level lists; only the primitive work is shared.  The reference
+ * evaluates every shell quartet from its own primitives (aointegrals_contract.h:133-140).
+ * The schedule is kept (cqg_autotune_next retunes it for the changed lists); a CUDA graph
+ * captured before the change must be captured again. */
+cqg_status cqg_set_siblings(cqg_ctx *ctx, int on);
+cqg_status cqg_get_siblings(cqg_ctx *ctx, int *on);
+/* Sibling class k: a pair of sibling groups becomes one sibling entry when it holds at least
+ * min_members member quartets (2..16; default half of the class's sibling form, 8 for
+ * (ss|ss)); the member quartets of smaller pairs of groups are pair entries. */
+cqg_status cqg_set_sibling_min(cqg_ctx *ctx, int k, int min_members);
+
 /* Statistics of the last contraction (synchronises the context's stream). */
 cqg_status cqg_get_stats(cqg_ctx *ctx, cqg_stats *out);
-/* Largest number of quartets held in the device quartet list at once (8 bytes each;
- * default 2^32, 32 GiB).  Larger screened sets are filled and evaluated in chunks. */
+/* Largest number of entries held in the device quartet list at once (10 bytes each;
+ * default 2^32, 40 GiB; an entry is one quartet, or one sibling-group quartet).  Larger
+ * screened sets are filled and evaluated in chunks. */
 cqg_status cqg_set_list_budget(cqg_ctx *ctx, long long quartets);
 /* Per-class kernel timing on (1) / off (0, default). */
 cqg_status cqg_set_timing(cqg_ctx *ctx, int on);
 /* Name of quartet class index k ("(pp|ps)"), or NULL past the last class. */
 const char *cqg_class_name(int k);
+/* Work lists of the schedule arrays (cqg_get_schedule / cqg_set_schedule /
+ * cqg_get_launch_shapes): 4 x 55 = 220, list b = part * 55 + class, parts: the FP64 and the
+ * FP32 pair entries of each class, then its FP64 and FP32 sibling entries (cqg_set_siblings;
+ * empty for the classes without them).  cqg_list_class gives list b's quartet class (-1 out
+ * of range). */
+int cqg_schedule_lists(void);
+int cqg_list_class(int b);
 
 /* ---- Kernels of the learned initial-density model (csrc/mlp.cu) ----
  * BF16 operands, FP32 accumulation; all pointers are device pointers, work is enqueued on

@@ -86,3 +86,27 @@ def test_mixed_phase_threshold_is_loosened_then_restored():
     tight.precision, tight.fp32_cutoff, tight.incremental, tight.mixed_threshold = "mixed", 1e-8, True, None
     assert abs(tight.SCF3() - E64) < 1e-8
     ref.close()
+
+
+def test_mixed_sibling_lists_match_pair_lists():
+    """FP32 sibling-group lists: the same FP32 quartet set as the pair-level lists, and the
+    same bound on the difference from the FP64 build."""
+    from chronusq_public_b200.aointegrals import AOIntegrals, PREC_MIXED
+    mol = water_cluster(4, 21)
+    bs = BasisSet("cc-pvdz", mol.atoms, mol.coords)
+    ints = AOIntegrals(bs)
+    ints.setSiblings(True)
+    D = _rand_density(bs.nbasis, 5)
+    G64, _ = ints.formPT(D)
+    cutoff = 1e-7
+    ints.setPrecision(PREC_MIXED, cutoff)
+    Gon, _ = ints.formPT(D)
+    st_on = ints.stats()
+    ints.setSiblings(False)
+    Goff, _ = ints.formPT(D)
+    st_off = ints.stats()
+    assert st_on["quartets_fp32"] == st_off["quartets_fp32"] > 0
+    assert st_on["quartets"] == st_off["quartets"]
+    assert "(ss|ss)" in st_on["sibling_classes"]
+    assert np.abs(Gon - G64).max() < 50 * cutoff
+    assert np.abs(Goff - G64).max() < 50 * cutoff

@@ -286,3 +286,67 @@ def test_autotuner_picks_a_fusion_tier_and_keeps_parity():
     Gr, _, _ = O.form_pt(ob, D)
     assert np.abs(G1 - Gr).max() <= TOL_G and np.abs(G2 - Gr).max() <= TOL_G
     ints.close()
+
+
+@pytest.mark.parametrize("basis,nwater,seed", [("cc-pvdz", 3, 11), ("cc-pvtz", 2, 17), ("6-31g*", 3, 5)])
+def test_sibling_groups_match_pair_lists_and_oracle(basis, nwater, seed):
+    """Sibling-group lists (pairs of the segmented shells of one general contraction share
+    their primitive pairs) give the oracle's G and quartet count and the pair-level lists'
+    per-class counts (RHF and UHF lists).  cc-pVXZ oxygen's 1s and 2s shells are siblings,
+    so fewer list entries and fewer primitive quartets are evaluated; 6-31G(d) has no
+    siblings of one angular momentum, so its sibling lists stay empty."""
+    mol = water_cluster(nwater, seed)
+    bs = BasisSet(basis, mol.atoms, mol.coords)
+    ob = O.OracleBasis.from_basis(bs)
+    Ps = rand_sym(bs.nbasis, 61)
+    Pz = rand_sym(bs.nbasis, 62, 0.2)
+    ints = _aoi()(bs)
+    ints.setSiblings(True)
+    assert ints.siblings()
+    on = ints.formPT(Ps, Pz)
+    st_on = ints.stats()
+    ints.setSiblings(False)
+    assert not ints.siblings()
+    off = ints.formPT(Ps, Pz)
+    st_off = ints.stats()
+    PTs_r, PTz_r, nr = O.form_pt(ob, Ps, Pz)
+    assert st_on["quartets"] == st_off["quartets"] == nr
+    assert st_on["class_quartets"] == st_off["class_quartets"]
+    for (PTs, PTz) in (on, off):
+        assert np.abs(PTs - PTs_r).max() <= TOL_G
+        assert np.abs(PTz - PTz_r).max() <= TOL_G
+    assert np.abs(on[0] - off[0]).max() <= 1e-12 and np.abs(on[1] - off[1]).max() <= 1e-12
+    assert st_off["sibling_classes"] == [] and st_off["list_entries"] == st_off["quartets"]
+    if basis == "6-31g*":
+        assert st_on["sibling_classes"] == [] and st_on["list_entries"] == st_on["quartets"]
+    else:
+        assert "(ss|ss)" in st_on["sibling_classes"] and "(ps|ss)" in st_on["sibling_classes"]
+        assert st_on["list_entries"] < st_off["list_entries"]
+        assert st_on["prim_quartets"] < st_off["prim_quartets"]
+        assert st_on["model_flops"] == pytest.approx(st_off["model_flops"], rel=1e-12)
+    ints.close()
+
+
+def test_sibling_groups_under_forced_schedules_chunks_and_fusion():
+    """The sibling lists through several quartets claimed per warp, a list budget that
+    forces chunked fill/evaluate passes, and the class-fused kernel beside them."""
+    mol = water_cluster(3, 7)
+    bs = BasisSet("cc-pvdz", mol.atoms, mol.coords)
+    ob = O.OracleBasis.from_basis(bs)
+    D = rand_sym(bs.nbasis, 63)
+    Gr, _, nr = O.form_pt(ob, D)
+    ints = _aoi()(bs)
+    ints.setSiblings(True)
+    ints.setSchedule(cta_per_sm=8, quartets_per_warp=4)
+    G1, _ = ints.formPT(D)
+    assert ints.stats()["quartets"] == nr and np.abs(G1 - Gr).max() <= TOL_G
+    ints.setListBudget(20000)
+    G2, _ = ints.formPT(D)
+    st = ints.stats()
+    assert st["chunks"] > 1 and st["quartets"] == nr and np.abs(G2 - Gr).max() <= TOL_G
+    ints.setListBudget(1 << 32)
+    for tier in (1, 2):
+        ints.setFusion(tier)
+        G3, _ = ints.formPT(D)
+        assert ints.stats()["quartets"] == nr and np.abs(G3 - Gr).max() <= TOL_G, tier
+    ints.close()
