@@ -81,10 +81,10 @@ static void pair_prims(const cqg_ctx *ctx, int a, int b, double prim_thresh, std
 
 // primitive-count bucket of a shell pair: warps of the ERI kernels see kets of one bucket
 static inline int prim_bucket(int np) {
-  static const int upper[CQG_NPBUCKET - 1] = {1, 2, 3, 4, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64};
-  for (int b = 0; b < CQG_NPBUCKET - 1; ++b)
+  static const int upper[CQG_NBUCKET - 1] = {1, 2, 3, 4, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64};
+  for (int b = 0; b < CQG_NBUCKET - 1; ++b)
     if (np <= upper[b]) return b;
-  return CQG_NPBUCKET - 1;
+  return CQG_NBUCKET - 1;
 }
 
 // build primitive-pair data for the current pair ordering and upload all pair arrays
@@ -643,7 +643,7 @@ cqg_status cqg_set_basis_batch(cqg_ctx *ctx, int nmol, const int *nshell_per_mol
   const int npairs = (int)ctx->pair_sh.size();
   const std::vector<int> fam = cqg_sib::shell_families(nshell, L, nprim, ctx->hpoff.data(), alpha, centers,
                                                        ctx->hshmol.data());
-  std::vector<int> pgid(npairs), prank(npairs), gnp_of(npairs), gsz_of(npairs);   // *_of: by group id
+  std::vector<int> pgid(npairs), prank(npairs), gnp_of(npairs);   // gnp_of: by group id
   std::vector<double> gq_of(npairs, 0.0);
   {
     int gbase = 0;
@@ -672,21 +672,17 @@ cqg_status cqg_set_basis_batch(cqg_ctx *ctx, int nmol, const int *nshell_per_mol
       double q = 0.0;
       for (int i : members[g]) q = std::max(q, ctx->pair_Q[i]);
       gq_of[g] = q;
-      gsz_of[g] = (int)members[g].size();
       tmp.clear();
       w.clear();
       group_prims(ctx, members[g].data(), (int)members[g].size(), 1, 1e-24, fam, tmp, w);
       gnp_of[g] = (int)tmp.size();
     }
   }
-  // Sort each class by (molecule, bucket of the group, group Q descending, group, member),
-  // stable; the bucket is (one member or more, primitive-count bucket).  The members of a
-  // group become consecutive pairs led by the first, and Qc (the group's Q) is
-  // non-increasing within each bucket.  Per (molecule, class) bucket starts -> molbk (pair
-  // index) and molgbk (group index).
-  auto bucket_of = [&](int i) {
-    return (gsz_of[pgid[i]] > 1 ? CQG_NPBUCKET : 0) + prim_bucket(gnp_of[pgid[i]]);
-  };
+  // Sort each class by (molecule, primitive-count bucket of the group, group Q descending,
+  // group, member), stable.  The members of a group become consecutive pairs led by the
+  // first, and Qc (the group's Q) is non-increasing within each bucket.  Per (molecule,
+  // class) bucket starts -> molbk (pair index) and molgbk (group index).
+  auto bucket_of = [&](int i) { return prim_bucket(gnp_of[pgid[i]]); };
   const int NB1 = CQG_NBUCKET + 1;
   std::vector<int> molbk((size_t)nmol * CQG_NPC * NB1, 0), molgbk((size_t)nmol * CQG_NPC * NB1, 0);
   std::vector<int> new_gid(npairs);
@@ -836,7 +832,11 @@ static cqg_status autotune_shapes(cqg_ctx *ctx, const long long *crange, cudaStr
     };
     // (CTAs per SM, warps per CTA, quartets claimed per warp, kernel form)
     std::vector<Shape> cand;
-    if (!warp) {
+    if (sibling) {   // sibling lists: also CTAs of 64 threads (2 warps)
+      for (int w : {2, 4})
+        for (int c : {4, 8, 16})
+          for (int q : {1, 4}) cand.push_back({c, w, q, 0});
+    } else if (!warp) {
       for (int c : {4, 8, 12, 16, 24})
         for (int q : {1, 4}) cand.push_back({c, 0, q, 0});
     }

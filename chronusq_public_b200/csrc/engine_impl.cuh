@@ -30,11 +30,7 @@
 #define CQG_NPC ((CQG_MAXL + 1) * (CQG_MAXL + 2) / 2)       // pair classes
 #define CQG_NQC (CQG_NPC * (CQG_NPC + 1) / 2)                // quartet classes
 #define CQG_MAXG 4
-// Ket buckets of a (molecule, pair class): the primitive-count bucket of the pair's group,
-// and whether the group has one member (kind 0) or more (kind 1):
-// bucket = kind * CQG_NPBUCKET + primitive bucket.
-#define CQG_NPBUCKET 16
-#define CQG_NBUCKET (2 * CQG_NPBUCKET)
+#define CQG_NBUCKET 16   // ket buckets of a (molecule, pair class): the primitive-count bucket of the pair's group
 
 static_assert(CQG_NQC <= 55, "class table");
 
@@ -350,6 +346,212 @@ __device__ __forceinline__ unsigned warp_excl_scan(unsigned x, unsigned &total) 
 // the contracted quartets, their count and their precision are those of the pair-level
 // lists.  In a diagonal block (bra class = ket class) ket group <= bra group, and within one
 // group ket member <= bra member, so every unordered pair of pairs is taken once.
+//
+// Tasks take the class's bra pairs (groups) from the last: the pairs are ordered by
+// primitive-count bucket, so each class list starts with its heaviest quartets and the
+// work queues hand out the light ones at the end of a launch.
+struct ScreenTally {
+  unsigned long long km64 = 0, ke64 = 0, km32 = 0, ke32 = 0, nq64 = 0, nq32 = 0;
+};
+
+template <bool FILL>
+__device__ __forceinline__ void screen_pair_task(const BlockTable &bt, int blk, int t, const Pairs &P,
+                                                 const double *__restrict__ M, const double *__restrict__ MT,
+                                                 const double *__restrict__ Mpair, const Mols &mols,
+                                                 const int *__restrict__ shmol, double mm, double thresh,
+                                                 double cut32, const bool (&dop)[kListParts],
+                                                 const long long (&base)[kListParts], long long (&cpart)[kListParts],
+                                                 uint2 *__restrict__ qlist, long long cap, ScreenTally &ty) {
+  const int lane = threadIdx.x & 31;
+  const int bra = bt.bra_beg[blk] + t;
+  const double qb = P.Q[bra];
+  if (!(qb * mm > 0.0)) return;
+  const double cut = thresh / (qb * mm) * (1.0 - 1e-12);
+  const int2 ab = P.sh[bra];
+  const int mol = shmol[ab.x];
+  if (!mols.active[mol]) return;
+  const int nsh = mols.nsh[mol], shoff = mols.shoff[mol];
+  const double *Mm = M + mols.Moff[mol];
+  const double *col1 = MT + mols.Moff[mol] + (size_t)(ab.x - shoff) * nsh;
+  const double *col2 = MT + mols.Moff[mol] + (size_t)(ab.y - shoff) * nsh;
+  const double m12 = Mm[(ab.x - shoff) + (size_t)(ab.y - shoff) * nsh];
+  const int *bkt = mols.molbk + ((size_t)mol * CQG_NPC + bt.ket_class[blk]) * (CQG_NBUCKET + 1);
+  const unsigned long long kkb = (unsigned long long)P.kk[bra], npb = (unsigned long long)P.np[bra];
+  const unsigned below = (1u << lane) - 1u;
+  for (int bk = 0; bk < CQG_NBUCKET; ++bk) {
+    const int kb = bkt[bk], ke = bkt[bk + 1];
+    if (ke <= kb) continue;
+    int kend = kb + coarse_range(P.Qc, kb, ke - kb, cut);
+    if (bt.diag[blk]) kend = min(kend, bra + 1);   // unique pairs of pairs: ket <= bra
+    for (int k0 = kb; k0 < kend; k0 += 32) {
+      const int ket = k0 + lane;
+      bool hi = false, lo = false;
+      if (ket < kend) {
+        const double bnd = quartet_bound(col1, col2, m12, Mpair[ket], shoff, P.sh[ket], qb, P.Q[ket]);
+        const bool pass = bnd >= thresh;
+        lo = pass && bnd < cut32;
+        hi = pass && !lo;
+      }
+      const unsigned b64 = __ballot_sync(0xffffffffu, hi), b32 = __ballot_sync(0xffffffffu, lo);
+      if (FILL) {
+        if (hi && dop[0]) {
+          const long long pos = base[0] + cpart[0] + __popc(b64 & below);
+          if (pos < cap) qlist[pos] = make_uint2((unsigned)bra, (unsigned)ket);
+        }
+        if (lo && dop[1]) {
+          const long long pos = base[1] + cpart[1] + __popc(b32 & below);
+          if (pos < cap) qlist[pos] = make_uint2((unsigned)bra, (unsigned)ket);
+        }
+      } else {
+        if (hi) {
+          ty.km64 += (unsigned long long)P.kk[ket];
+          ty.ke64 += (unsigned long long)P.np[ket];
+        }
+        if (lo) {
+          ty.km32 += (unsigned long long)P.kk[ket];
+          ty.ke32 += (unsigned long long)P.np[ket];
+        }
+      }
+      cpart[0] += __popc(b64);
+      cpart[1] += __popc(b32);
+    }
+  }
+  if (!FILL) {   // the bra's factors are common to the task's quartets
+    ty.km64 *= kkb;
+    ty.ke64 *= npb;
+    ty.km32 *= kkb;
+    ty.ke32 *= npb;
+    ty.nq64 = (unsigned long long)cpart[0];
+    ty.nq32 = (unsigned long long)cpart[1];
+  }
+}
+
+template <bool FILL>
+__device__ __forceinline__ void screen_group_task(const BlockTable &bt, int blk, int t, const Pairs &P,
+                                                  const double *__restrict__ MT, const double *__restrict__ Mpair,
+                                                  const Mols &mols, const int *__restrict__ shmol, double mm,
+                                                  double thresh, double cut32, const bool (&dop)[kListParts],
+                                                  const long long (&base)[kListParts],
+                                                  long long (&cpart)[kListParts], uint2 *__restrict__ qlist,
+                                                  unsigned short *__restrict__ qmask, long long cap,
+                                                  ScreenTally &ty) {
+  const int lane = threadIdx.x & 31;
+  const int gbra = bt.gbra_beg[blk] + t;
+  const int bra = P.glead[gbra];
+  const int mb = P.gsz[bra];
+  const int min_members = bt.min_members[blk];
+  const double qb = P.gQ[gbra];
+  if (!(qb * mm > 0.0)) return;
+  const double cut = thresh / (qb * mm) * (1.0 - 1e-12);
+  const double tcut = thresh * (1.0 - 1e-12);   // margin for the rounding of the Q products
+  const int mol = shmol[P.sh[bra].x];
+  if (!mols.active[mol]) return;
+  const int nsh = mols.nsh[mol], shoff = mols.shoff[mol];
+  const double *MTm = MT + mols.Moff[mol];
+  const int *bkt = mols.molgbk + ((size_t)mol * CQG_NPC + bt.ket_class[blk]) * (CQG_NBUCKET + 1);
+  const unsigned below = (1u << lane) - 1u;
+  for (int bk = 0; bk < CQG_NBUCKET; ++bk) {
+    const int kb = bkt[bk], ke = bkt[bk + 1];
+    if (ke <= kb) continue;
+    int kend = kb + coarse_range(P.gQ, kb, ke - kb, cut);
+    if (bt.diag[blk]) kend = min(kend, gbra + 1);   // ket group <= bra group
+    for (int k0 = kb; k0 < kend; k0 += 32) {
+      const int kx = k0 + lane;   // ket group
+      int ket = 0;
+      unsigned m64 = 0, m32 = 0;  // member masks, bit 4 i + j
+      bool sib = false;
+      if (kx < kend) {
+        ket = P.glead[kx];
+        const int mk = P.gsz[ket];
+        const bool same = bt.diag[blk] && kx == gbra;
+        sib = mb * mk > 1 && (same ? mb * (mb + 1) / 2 : mb * mk) >= min_members;
+        const double qk = P.gQ[kx];
+        for (int i = 0; i < mb; ++i) {
+          const int bi = bra + i;
+          const double qi = P.Q[bi];
+          // the bound of each member quartet is at most Mmax Q_i Q_j: skip the six norms where
+          // that already falls short (the groups' coarse range holds their largest Q)
+          if (qi * qk * mm < tcut) continue;
+          const int2 abi = P.sh[bi];
+          const double *c1 = MTm + (size_t)(abi.x - shoff) * nsh;
+          const double *c2 = MTm + (size_t)(abi.y - shoff) * nsh;
+          const double mi = Mpair[bi];
+          const int jmax = same ? min(mk, i + 1) : mk;
+          for (int j = 0; j < jmax; ++j) {
+            const int kj = ket + j;
+            const double qj = P.Q[kj];
+            if (qi * qj * mm < tcut) continue;
+            const double bnd = quartet_bound(c1, c2, mi, Mpair[kj], shoff, P.sh[kj], qi, qj);
+            if (bnd < thresh) continue;
+            const unsigned bit = 1u << (4 * i + j);
+            if (bnd < cut32) m32 |= bit; else m64 |= bit;
+            if (!FILL) {
+              const unsigned long long kq = (unsigned long long)P.kk[bi] * (unsigned long long)P.kk[kj];
+              // executed primitive quartets of a member quartet evaluated on its own
+              const unsigned long long eq =
+                  sib ? 0ull : (unsigned long long)P.np[bi] * (unsigned long long)P.np[kj];
+              if (bnd < cut32) {
+                ty.km32 += kq;
+                ty.ke32 += eq;
+              } else {
+                ty.km64 += kq;
+                ty.ke64 += eq;
+              }
+            }
+          }
+        }
+        if (!FILL) {
+          if (sib) {   // a sibling entry evaluates the groups' shared primitive pairs once
+            const unsigned long long gq = (unsigned long long)P.gnp[bra] * (unsigned long long)P.gnp[ket];
+            if (m64) ty.ke64 += gq;
+            if (m32) ty.ke32 += gq;
+          }
+          ty.nq64 += (unsigned long long)__popc(m64);
+          ty.nq32 += (unsigned long long)__popc(m32);
+        }
+      }
+      // pair entries (one per member quartet) of parts 0 and 1: several per lane
+      const unsigned n0 = sib ? 0u : (unsigned)__popc(m64), n1 = sib ? 0u : (unsigned)__popc(m32);
+      unsigned t0, t1;
+      const unsigned e0 = warp_excl_scan(n0, t0), e1 = warp_excl_scan(n1, t1);
+      // sibling entries of parts 2 and 3: at most one per lane
+      const unsigned b2 = __ballot_sync(0xffffffffu, sib && m64), b3 = __ballot_sync(0xffffffffu, sib && m32);
+      if (FILL) {
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+          unsigned m = p == 0 ? (sib ? 0u : m64) : (sib ? 0u : m32);
+          if (!m || !dop[p]) continue;
+          long long pos = base[p] + cpart[p] + (p == 0 ? e0 : e1);
+          while (m) {   // member quartets in bit order
+            const int bit = __ffs(m) - 1;
+            m &= m - 1;
+            if (pos < cap) qlist[pos] = make_uint2((unsigned)(bra + (bit >> 2)), (unsigned)(ket + (bit & 3)));
+            ++pos;
+          }
+        }
+        if (sib && m64 && dop[2]) {
+          const long long pos = base[2] + cpart[2] + __popc(b2 & below);
+          if (pos < cap) {
+            qlist[pos] = make_uint2((unsigned)bra, (unsigned)ket);
+            qmask[pos] = (unsigned short)m64;
+          }
+        }
+        if (sib && m32 && dop[3]) {
+          const long long pos = base[3] + cpart[3] + __popc(b3 & below);
+          if (pos < cap) {
+            qlist[pos] = make_uint2((unsigned)bra, (unsigned)ket);
+            qmask[pos] = (unsigned short)m32;
+          }
+        }
+      }
+      cpart[0] += t0;
+      cpart[1] += t1;
+      cpart[2] += __popc(b2);
+      cpart[3] += __popc(b3);
+    }
+  }
+}
+
 template <bool FILL>
 __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pairs P, const double *__restrict__ M,
                                                   const double *__restrict__ MT, const double *__restrict__ Mpair,
@@ -360,8 +562,8 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
                                                   unsigned short *__restrict__ qmask,
                                                   unsigned long long *__restrict__ blkacc, long long vt0,
                                                   long long vt1, long long obase, long long cap) {
-  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   if (warp >= ntask) return;
   // fill pass: only the parts (virtual tasks part * ntask + warp) inside the chunk
   bool dop[kListParts];
@@ -374,168 +576,47 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
   }
   if (FILL && !any) return;
   const int blk = find_block(bt, warp);
-  const bool grouped = bt.grouped[blk] != 0;
-  // Tasks take the class's bra pairs (groups) from the last: the pairs are ordered by
-  // primitive-count bucket, so the list starts with the heaviest quartets and the work
-  // queues hand out the light ones at the end of a launch.
-  const int t = bt.task_beg[blk + 1] - 1 - warp;
-  const int gbra = grouped ? bt.gbra_beg[blk] + t : -1;
-  const int bra = grouped ? P.glead[gbra] : bt.bra_beg[blk] + t;
-  const int mb = grouped ? P.gsz[bra] : 1;
-  const int min_members = bt.min_members[blk];
-  const double qb = grouped ? P.gQ[gbra] : P.Q[bra];
-  double mm = *Mmax;
-  double cut = (qb * mm > 0.0) ? thresh / (qb * mm) * (1.0 - 1e-12) : 0.0;
-  int2 ab = P.sh[bra];
-  const int mol = shmol[ab.x];
-  const int nsh = mols.nsh[mol], shoff = mols.shoff[mol];
-  const double *Mm = M + mols.Moff[mol];
-  const double *MTm = MT + mols.Moff[mol];
-  const double *col1 = MTm + (size_t)(ab.x - shoff) * nsh;
-  const double *col2 = MTm + (size_t)(ab.y - shoff) * nsh;
-  const double m12 = Mm[(ab.x - shoff) + (size_t)(ab.y - shoff) * nsh];
-  const int *bkt = (grouped ? mols.molgbk : mols.molbk) + ((size_t)mol * CQG_NPC + bt.ket_class[blk]) * (CQG_NBUCKET + 1);
-  const double *Qs = grouped ? P.gQ : P.Qc;   // non-increasing within each bucket
+  const int t = bt.task_beg[blk + 1] - 1 - warp;   // heaviest bra first
   long long base[kListParts], cpart[kListParts];
 #pragma unroll
   for (int p = 0; p < kListParts; ++p) {
     base[p] = FILL ? off[(long long)p * ntask + warp] - obase : 0;
     cpart[p] = 0;
   }
-  unsigned long long km64 = 0, ke64 = 0, km32 = 0, ke32 = 0, nq64 = 0, nq32 = 0;
-  if (qb * mm > 0.0 && mols.active[mol]) {
-    for (int bk = 0; bk < CQG_NBUCKET; ++bk) {
-      const int kb = bkt[bk], ke = bkt[bk + 1];
-      if (ke <= kb) continue;
-      int kend = kb + coarse_range(Qs, kb, ke - kb, cut);
-      if (bt.diag[blk]) kend = min(kend, (grouped ? gbra : bra) + 1);   // unique pairs of pairs
-      for (int k0 = kb; k0 < kend; k0 += 32) {
-        const int kx = k0 + lane;   // ket pair, or ket group in a grouped block
-        int ket = 0;
-        unsigned m64 = 0, m32 = 0;   // member masks (bit 4 i + j); pair blocks: bit 0
-        bool sib = false;            // grouped: the pair of groups is one sibling entry
-        if (kx < kend) {
-          if (!grouped) {
-            ket = kx;
-            const double bnd = quartet_bound(col1, col2, m12, Mpair[ket], shoff, P.sh[ket], qb, P.Q[ket]);
-            if (bnd >= thresh) {
-              if (bnd < cut32) m32 = 1u; else m64 = 1u;
-            }
-            if (!FILL && m64) {
-              km64 += (unsigned long long)P.kk[ket] * (unsigned long long)P.kk[bra];
-              ke64 += (unsigned long long)P.np[ket] * (unsigned long long)P.np[bra];
-            }
-            if (!FILL && m32) {
-              km32 += (unsigned long long)P.kk[ket] * (unsigned long long)P.kk[bra];
-              ke32 += (unsigned long long)P.np[ket] * (unsigned long long)P.np[bra];
-            }
-          } else {
-            ket = P.glead[kx];
-            const int mk = P.gsz[ket];
-            const bool same = bt.diag[blk] && kx == gbra;
-            sib = mb * mk > 1 && (same ? mb * (mb + 1) / 2 : mb * mk) >= min_members;
-            for (int i = 0; i < mb; ++i) {
-              const int bi = bra + i;
-              const int2 abi = P.sh[bi];
-              const double *c1 = MTm + (size_t)(abi.x - shoff) * nsh;
-              const double *c2 = MTm + (size_t)(abi.y - shoff) * nsh;
-              const double mi = Mpair[bi], qi = P.Q[bi];
-              const int jmax = same ? min(mk, i + 1) : mk;
-              for (int j = 0; j < jmax; ++j) {
-                const int kj = ket + j;
-                const double bnd = quartet_bound(c1, c2, mi, Mpair[kj], shoff, P.sh[kj], qi, P.Q[kj]);
-                if (bnd < thresh) continue;
-                const unsigned bit = 1u << (4 * i + j);
-                const unsigned long long kq = (unsigned long long)P.kk[bi] * (unsigned long long)P.kk[kj];
-                // executed primitive quartets of a member quartet evaluated on its own
-                const unsigned long long eq =
-                    sib ? 0ull : (unsigned long long)P.np[bi] * (unsigned long long)P.np[kj];
-                if (bnd < cut32) {
-                  m32 |= bit;
-                  if (!FILL) {
-                    km32 += kq;
-                    ke32 += eq;
-                  }
-                } else {
-                  m64 |= bit;
-                  if (!FILL) {
-                    km64 += kq;
-                    ke64 += eq;
-                  }
-                }
-              }
-            }
-            if (!FILL && sib) {   // a sibling entry evaluates the groups' shared primitive pairs once
-              const unsigned long long gq = (unsigned long long)P.gnp[bra] * (unsigned long long)P.gnp[ket];
-              if (m64) ke64 += gq;
-              if (m32) ke32 += gq;
-            }
-          }
-        }
-        if (!FILL) {
-          nq64 += (unsigned long long)__popc(m64);
-          nq32 += (unsigned long long)__popc(m32);
-        }
-        // entries of this lane per part: pair entries one per member quartet, sibling entries one per mask
-        unsigned n[kListParts];
-        n[0] = sib ? 0u : (unsigned)__popc(m64);
-        n[1] = sib ? 0u : (unsigned)__popc(m32);
-        n[2] = (sib && m64) ? 1u : 0u;
-        n[3] = (sib && m32) ? 1u : 0u;
-#pragma unroll
-        for (int p = 0; p < kListParts; ++p) {
-          unsigned total, before;
-          if (grouped && p < 2) {   // several pair entries per lane
-            before = warp_excl_scan(n[p], total);
-          } else {                  // at most one entry per lane
-            const unsigned b = __ballot_sync(0xffffffffu, n[p] != 0);
-            before = __popc(b & ((1u << lane) - 1u));
-            total = __popc(b);
-          }
-          if (FILL && dop[p] && n[p]) {
-            long long pos = base[p] + cpart[p] + before;
-            if (p >= 2) {
-              if (pos < cap) {
-                qlist[pos] = make_uint2((unsigned)bra, (unsigned)ket);
-                qmask[pos] = (unsigned short)(p == 2 ? m64 : m32);
-              }
-            } else {
-              unsigned m = p == 0 ? m64 : m32;
-              while (m) {   // member quartets in bit order
-                const int bit = __ffs(m) - 1;
-                m &= m - 1;
-                if (pos < cap) qlist[pos] = make_uint2((unsigned)(bra + (bit >> 2)), (unsigned)(ket + (bit & 3)));
-                ++pos;
-              }
-            }
-          }
-          cpart[p] += total;
-        }
-      }
-    }
-  }
+  ScreenTally ty;
+  const double mm = *Mmax;
+  if (bt.grouped[blk])
+    screen_group_task<FILL>(bt, blk, t, P, MT, Mpair, mols, shmol, mm, thresh, cut32, dop, base, cpart, qlist,
+                            qmask, cap, ty);
+  else
+    screen_pair_task<FILL>(bt, blk, t, P, M, MT, Mpair, mols, shmol, mm, thresh, cut32, dop, base, cpart, qlist,
+                           cap, ty);
   if (!FILL) {
     for (int o = 16; o > 0; o >>= 1) {
-      km64 += __shfl_xor_sync(0xffffffffu, km64, o);
-      ke64 += __shfl_xor_sync(0xffffffffu, ke64, o);
-      km32 += __shfl_xor_sync(0xffffffffu, km32, o);
-      ke32 += __shfl_xor_sync(0xffffffffu, ke32, o);
-      nq64 += __shfl_xor_sync(0xffffffffu, nq64, o);
-      nq32 += __shfl_xor_sync(0xffffffffu, nq32, o);
+      ty.km64 += __shfl_xor_sync(0xffffffffu, ty.km64, o);
+      ty.ke64 += __shfl_xor_sync(0xffffffffu, ty.ke64, o);
+      ty.km32 += __shfl_xor_sync(0xffffffffu, ty.km32, o);
+      ty.ke32 += __shfl_xor_sync(0xffffffffu, ty.ke32, o);
+    }
+    if (bt.grouped[blk]) {   // pair tasks count whole warps already
+      for (int o = 16; o > 0; o >>= 1) {
+        ty.nq64 += __shfl_xor_sync(0xffffffffu, ty.nq64, o);
+        ty.nq32 += __shfl_xor_sync(0xffffffffu, ty.nq32, o);
+      }
     }
     if (lane == 0) {
 #pragma unroll
       for (int p = 0; p < kListParts; ++p) cnt[(long long)p * ntask + warp] = cpart[p];
       unsigned long long *acc = blkacc + kBlkAcc * blk;
-      if (nq64) {
-        atomicAdd(acc + 0, km64);
-        atomicAdd(acc + 1, ke64);
-        atomicAdd(acc + 4, nq64);
+      if (ty.nq64) {
+        atomicAdd(acc + 0, ty.km64);
+        atomicAdd(acc + 1, ty.ke64);
+        atomicAdd(acc + 4, ty.nq64);
       }
-      if (nq32) {
-        atomicAdd(acc + 2, km32);
-        atomicAdd(acc + 3, ke32);
-        atomicAdd(acc + 5, nq32);
+      if (ty.nq32) {
+        atomicAdd(acc + 2, ty.km32);
+        atomicAdd(acc + 3, ty.ke32);
+        atomicAdd(acc + 5, ty.nq32);
       }
     }
   }
@@ -826,9 +907,10 @@ __device__ __forceinline__ void eri_jk_one(const uint2 *__restrict__ ql, long lo
 }
 
 // Sibling-group list of class (LA LB|LC LD): the work queue and persistent grid of
-// k_eri_jk, one entry (bra group, ket group, member mask) per thread.
-template <int LA, int LB, int LC, int LD, typename T>
-__global__ void __launch_bounds__(kEriThreads) k_eri_gc(const uint2 *__restrict__ ql, const long long *__restrict__ range,
+// k_eri_jk, one entry (bra group, ket group, member mask) per thread, NT threads per CTA
+// (64 lets one more CTA of these register-heavy kernels reside on an SM).
+template <int LA, int LB, int LC, int LD, typename T, int NT>
+__global__ void __launch_bounds__(NT) k_eri_gc(const uint2 *__restrict__ ql, const long long *__restrict__ range,
                                                 int blk, Pairs P, Shells S, const double *__restrict__ boys_g,
                                                 DigestGroups dg, unsigned long long *__restrict__ qhead, int chunk) {
   __shared__ __align__(16) double boys[BOYS_NT * BOYS_SROW];
@@ -1629,17 +1711,24 @@ static inline Mols make_mols(cqg_ctx *ctx) {
 
 typedef cudaError_t (*eri_launcher)(cqg_ctx *, int blk, long long n, cudaStream_t st, const DigestGroups &dg);
 
-// One launch of the sibling-group kernel of class (LA LB|LC LD) over list blk.
+// One launch of the sibling-group kernel of class (LA LB|LC LD) over list blk: CTAs of 64
+// threads when the list's schedule gives 2 warps per CTA, else 128.
 template <int LA, int LB, int LC, int LD, typename T>
 static cudaError_t launch_gc(cqg_ctx *ctx, int blk, long long n, cudaStream_t st, const DigestGroups &dg) {
   if (n == 0) return cudaSuccess;   // n < 0: count unknown on the host (graph mode)
+  const int nt = ctx->shape_wpb[blk] == 2 ? 64 : kEriThreads;
   const int cta = ctx->shape_cta[blk] > 0 ? ctx->shape_cta[blk] : 4;
   const long long cap = (long long)ctx->nsm * cta;
-  const long long nb = n > 0 ? std::min<long long>((n + kEriThreads - 1) / kEriThreads, cap) : cap;
+  const long long nb = n > 0 ? std::min<long long>((n + nt - 1) / nt, cap) : cap;
   const int chunk = 32 * (ctx->shape_qpw[blk] > 0 ? ctx->shape_qpw[blk] : 1);
-  k_eri_gc<LA, LB, LC, LD, T><<<(unsigned)nb, kEriThreads, 0, st>>>(ctx->d_qlist.p, ctx->d_range.p, blk,
-                                                                   make_pairs(ctx), make_shells(ctx), ctx->d_boys.p,
-                                                                   dg, ctx->d_qhead.p, chunk);
+  if (nt == 64)
+    k_eri_gc<LA, LB, LC, LD, T, 64><<<(unsigned)nb, 64, 0, st>>>(ctx->d_qlist.p, ctx->d_range.p, blk,
+                                                                make_pairs(ctx), make_shells(ctx), ctx->d_boys.p,
+                                                                dg, ctx->d_qhead.p, chunk);
+  else
+    k_eri_gc<LA, LB, LC, LD, T, kEriThreads><<<(unsigned)nb, kEriThreads, 0, st>>>(
+        ctx->d_qlist.p, ctx->d_range.p, blk, make_pairs(ctx), make_shells(ctx), ctx->d_boys.p, dg, ctx->d_qhead.p,
+        chunk);
   return cudaGetLastError();
 }
 

@@ -205,7 +205,8 @@ cqg_status cqg_get_launch_shapes(cqg_ctx *ctx, int *cta_per_sm, int *warps_per_c
 /* The same plus, per list, the work-queue chunk (the quartets one warp claims at a time:
  * per-thread kernels in units of 32, one per lane; warp-cooperative kernels one after the
  * other) and the kernel form (1 = warp-cooperative, 0 = one quartet per thread; classes
- * that have both forms get theirs from the autotuner).  Any output may be NULL; 0 in the
+ * that have both forms get theirs from the autotuner).  For the sibling-entry lists, warps
+ * per CTA 2 selects CTAs of 64 threads (otherwise 128).  Any output may be NULL; 0 in the
  * first three = default. */
 cqg_status cqg_get_schedule(cqg_ctx *ctx, int *cta_per_sm, int *warps_per_cta, int *quartets_per_warp,
                             int *warp_form);
