@@ -286,7 +286,8 @@ static cqg_status build_block_tables(cqg_ctx *ctx) {
   cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (long long *)nullptr, (long long *)nullptr,
                                 std::max<int>(kListParts * (int)task, 1));
   if (ctx->d_cnt.reserve(kListParts * task + 1) || ctx->d_off.reserve(kListParts * task + 1) ||
-      ctx->d_scan_tmp.reserve(scan_bytes + 16))
+      ctx->d_scan_tmp.reserve(scan_bytes + 16) || ctx->d_mslot.reserve(task + 1) || ctx->d_mhead.reserve(1) ||
+      ctx->d_masks.reserve(kMaskStepsInitial))
     return CQG_ERR_OOM;
   return CQG_OK;
 }
@@ -435,7 +436,7 @@ cqg_status cqg_destroy(cqg_ctx *ctx) {
   ctx->d_qlist.release(); ctx->d_G.release(); ctx->d_X.release(); ctx->d_AX.release(); ctx->d_Gscratch.release();
   ctx->d_molgbk.release(); ctx->d_gsz.release(); ctx->d_gpoff.release(); ctx->d_gnp.release(); ctx->d_gwoff.release();
   ctx->d_glead.release(); ctx->d_pair_Qc.release(); ctx->d_gQ.release(); ctx->d_gw.release(); ctx->d_gprim.release();
-  ctx->d_qmask.release();
+  ctx->d_qmask.release(); ctx->d_masks.release(); ctx->d_mhead.release(); ctx->d_mslot.release();
   if (ctx->events)
     for (int i = 0; i < 4 + 2 * CQG_NQC + 2; ++i) cudaEventDestroy(ctx->ev[i]);
   delete ctx;
@@ -959,6 +960,7 @@ static cqg_status contract_graph(cqg_ctx *ctx, int ngroups, const double *const 
   CUCHK(cudaMemsetAsync(ctx->d_flags.p, 0, 4 * sizeof(int), st));
   CUCHK(cudaMemsetAsync(ctx->d_Mmax.p, 0, sizeof(double), st));
   CUCHK(cudaMemsetAsync(ctx->d_blkacc.p, 0, kBlkAcc * CQG_NQC * sizeof(unsigned long long), st));
+  CUCHK(cudaMemsetAsync(ctx->d_mhead.p, 0, sizeof(unsigned long long), st));
   CUCHK(cudaMemsetAsync(ctx->d_G.p, 0, (size_t)ngroups * gsize * sizeof(double), st));
   {
     dim3 g((ctx->max_nsh + 127) / 128, ctx->max_nsh, ctx->nmol);
@@ -973,7 +975,7 @@ static cqg_status contract_graph(cqg_ctx *ctx, int ngroups, const double *const 
   const int nb = (ctx->ntask + 7) / 8;
   k_quartets<false><<<nb, 256, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, ctx->d_Mpair.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
                                          ctx->thresh, cut32, ctx->d_cnt.p, nullptr, nullptr, nullptr, ctx->d_blkacc.p,
-                                         0, 0, 0, 0);
+                                         0, 0, 0, 0, make_mask_cache(ctx));
   size_t scan_bytes = ctx->d_scan_tmp.n;
   CUCHK(cub::DeviceScan::ExclusiveSum(ctx->d_scan_tmp.p, scan_bytes, ctx->d_cnt.p, ctx->d_off.p,
                                       kListParts * ctx->ntask, st));
@@ -982,7 +984,8 @@ static cqg_status contract_graph(cqg_ctx *ctx, int ngroups, const double *const 
   k_quartets<true><<<nb, 256, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, ctx->d_Mpair.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
                                         ctx->thresh, cut32, nullptr, ctx->d_off.p, ctx->d_qlist.p, ctx->d_qmask.p,
                                         nullptr, 0,
-                                        (long long)kListParts * ctx->ntask, 0, ctx->graph_capacity);
+                                        (long long)kListParts * ctx->ntask, 0, ctx->graph_capacity,
+                                        make_mask_cache(ctx));
   CUCHK(cudaGetLastError());
   DigestGroups dg;
   memset(&dg, 0, sizeof(dg));
@@ -1037,6 +1040,17 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
   const Mols mols = make_mols(ctx);
   // Gh of every molecule: n x n for one molecule, packed per molecule for a batch
   const size_t gsize = ctx->nmol > 1 ? (size_t)ctx->packed : (size_t)n * n;
+  // the survivor-mask cache: grow it to what the last count pass asked for (tasks that did
+  // not fit tested their bounds twice), before this call's first launch; never in graph
+  // mode, whose captured launches hold the buffer's address
+  if (ctx->graph_capacity == 0 && ctx->mask_steps_used > (long long)ctx->d_masks.n) {
+    const long long want = std::min<long long>(ctx->mask_steps_used + ctx->mask_steps_used / 4, kMaskStepsMax);
+    if (want > (long long)ctx->d_masks.n && ctx->d_masks.reserve((size_t)want) != cudaSuccess &&
+        ctx->d_masks.reserve((size_t)kMaskStepsInitial) != cudaSuccess) {
+      ctx->err = "survivor-mask cache allocation failed";
+      return CQG_ERR_OOM;
+    }
+  }
   if (ctx->timing) CUCHK(cudaEventRecord(ctx->ev[0], st));
   // 1. block norms + checks
   XList xl;
@@ -1045,6 +1059,7 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
   CUCHK(cudaMemsetAsync(ctx->d_flags.p, 0, 4 * sizeof(int), st));
   CUCHK(cudaMemsetAsync(ctx->d_Mmax.p, 0, sizeof(double), st));
   CUCHK(cudaMemsetAsync(ctx->d_blkacc.p, 0, kBlkAcc * CQG_NQC * sizeof(unsigned long long), st));
+  CUCHK(cudaMemsetAsync(ctx->d_mhead.p, 0, sizeof(unsigned long long), st));
   const double cut32 = ctx->policy == CQG_PREC_MIXED ? ctx->fp32_cutoff : 0.0;
   ctx->launches = 0;
   {
@@ -1068,7 +1083,7 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
     k_quartets<false><<<nb, nthr, 0, st>>>(ctx->bt, ctx->ntask, P, ctx->d_M.p, ctx->d_M.p + ctx->Mtotal, ctx->d_Mpair.p, mols, ctx->d_shmol.p, ctx->d_Mmax.p,
                                             ctx->thresh,
                                             cut32, ctx->d_cnt.p, nullptr, nullptr, nullptr, ctx->d_blkacc.p, 0, 0, 0,
-                                            0);
+                                            0, make_mask_cache(ctx));
     CUCHK(cudaGetLastError());
     size_t scan_bytes = ctx->d_scan_tmp.n;
     CUCHK(cub::DeviceScan::ExclusiveSum(ctx->d_scan_tmp.p, scan_bytes, ctx->d_cnt.p, ctx->d_off.p,
@@ -1084,7 +1099,10 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
   CUCHK(cudaMemcpyAsync(hr, ctx->d_range.p, sizeof(hr), cudaMemcpyDeviceToHost, st));
   CUCHK(cudaMemcpyAsync(hacc, ctx->d_blkacc.p, sizeof(hacc), cudaMemcpyDeviceToHost, st));
   CUCHK(cudaMemcpyAsync(hflags, ctx->d_flags.p, sizeof(hflags), cudaMemcpyDeviceToHost, st));
+  unsigned long long hsteps = 0;
+  CUCHK(cudaMemcpyAsync(&hsteps, ctx->d_mhead.p, sizeof(hsteps), cudaMemcpyDeviceToHost, st));
   CUCHK(cudaStreamSynchronize(st));
+  ctx->mask_steps_used = (long long)hsteps;
   if (hflags[0]) {
     ctx->err = "input density contains NaN or Inf";
     return CQG_ERR_NONFINITE;
@@ -1202,7 +1220,8 @@ static cqg_status contract_device(cqg_ctx *ctx, int ngroups, const double *const
                                              ctx->thresh,
                                              cut32, nullptr, ctx->d_off.p, ctx->d_qlist.p, ctx->d_qmask.p, nullptr,
                                              vt0, vt1, obase,
-                                             (long long)std::min(ctx->d_qlist.n, ctx->d_qmask.n));
+                                             (long long)std::min(ctx->d_qlist.n, ctx->d_qmask.n),
+                                             make_mask_cache(ctx));
       CUCHK(cudaGetLastError());
       ctx->launches += 1;
     }

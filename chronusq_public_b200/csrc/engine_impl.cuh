@@ -354,22 +354,43 @@ struct ScreenTally {
   unsigned long long km64 = 0, ke64 = 0, km32 = 0, ke32 = 0, nq64 = 0, nq32 = 0;
 };
 
+// Survivor-mask cache between the two screening passes: the count pass stores, per task and
+// per 32-ket step, the FP64 and FP32 survivor ballots (one uint2) at the task's slot in
+// `masks`; the fill pass reads them instead of testing the bounds again.  A task whose
+// steps do not fit in the buffer gets slot -1 and the fill pass tests its bounds itself.
+static_assert(CQG_NBUCKET <= 32, "screen_pair_task searches one bucket per lane");
+constexpr long long kMaskStepsInitial = 1ll << 22;   // 32 MiB; grown to what a call used
+constexpr long long kMaskStepsMax = 1ll << 28;       // 2 GiB
+struct MaskCache {
+  uint2 *masks;
+  unsigned long long *head;   // next free step (zeroed before the count pass)
+  long long *slot;            // per task: first step, or -1
+  long long cap;              // steps the buffer holds
+};
+
 template <bool FILL>
-__device__ __forceinline__ void screen_pair_task(const BlockTable &bt, int blk, int t, const Pairs &P,
+__device__ __forceinline__ void screen_pair_task(const BlockTable &bt, int blk, int t, int task, const Pairs &P,
                                                  const double *__restrict__ M, const double *__restrict__ MT,
                                                  const double *__restrict__ Mpair, const Mols &mols,
                                                  const int *__restrict__ shmol, double mm, double thresh,
                                                  double cut32, const bool (&dop)[kListParts],
                                                  const long long (&base)[kListParts], long long (&cpart)[kListParts],
-                                                 uint2 *__restrict__ qlist, long long cap, ScreenTally &ty) {
+                                                 uint2 *__restrict__ qlist, long long cap, const MaskCache &mc,
+                                                 ScreenTally &ty) {
   const int lane = threadIdx.x & 31;
   const int bra = bt.bra_beg[blk] + t;
   const double qb = P.Q[bra];
-  if (!(qb * mm > 0.0)) return;
+  if (!(qb * mm > 0.0)) {
+    if (!FILL && lane == 0) mc.slot[task] = -1;
+    return;
+  }
   const double cut = thresh / (qb * mm) * (1.0 - 1e-12);
   const int2 ab = P.sh[bra];
   const int mol = shmol[ab.x];
-  if (!mols.active[mol]) return;
+  if (!mols.active[mol]) {
+    if (!FILL && lane == 0) mc.slot[task] = -1;
+    return;
+  }
   const int nsh = mols.nsh[mol], shoff = mols.shoff[mol];
   const double *Mm = M + mols.Moff[mol];
   const double *col1 = MT + mols.Moff[mol] + (size_t)(ab.x - shoff) * nsh;
@@ -378,21 +399,57 @@ __device__ __forceinline__ void screen_pair_task(const BlockTable &bt, int blk, 
   const int *bkt = mols.molbk + ((size_t)mol * CQG_NPC + bt.ket_class[blk]) * (CQG_NBUCKET + 1);
   const unsigned long long kkb = (unsigned long long)P.kk[bra], npb = (unsigned long long)P.np[bra];
   const unsigned below = (1u << lane) - 1u;
-  for (int bk = 0; bk < CQG_NBUCKET; ++bk) {
-    const int kb = bkt[bk], ke = bkt[bk + 1];
-    if (ke <= kb) continue;
-    int kend = kb + coarse_range(P.Qc, kb, ke - kb, cut);
-    if (bt.diag[blk]) kend = min(kend, bra + 1);   // unique pairs of pairs: ket <= bra
-    for (int k0 = kb; k0 < kend; k0 += 32) {
-      const int ket = k0 + lane;
-      bool hi = false, lo = false;
-      if (ket < kend) {
-        const double bnd = quartet_bound(col1, col2, m12, Mpair[ket], shoff, P.sh[ket], qb, P.Q[ket]);
-        const bool pass = bnd >= thresh;
-        lo = pass && bnd < cut32;
-        hi = pass && !lo;
+  // coarse range of every bucket at once: lane b < CQG_NBUCKET searches bucket b
+  int my_kb = 0, my_kend = 0;
+  if (lane < CQG_NBUCKET) {
+    const int kb = bkt[lane], ke = bkt[lane + 1];
+    int kend = kb;
+    if (ke > kb) {
+      kend = kb + coarse_range(P.Qc, kb, ke - kb, cut);
+      if (bt.diag[blk]) kend = min(kend, bra + 1);   // unique pairs of pairs: ket <= bra
+    }
+    my_kb = kb;
+    my_kend = max(kend, kb);
+  }
+  // the task's slot in the mask cache: the count pass reserves one step per 32 kets
+  long long slot = -1;
+  if (!FILL) {
+    unsigned steps;
+    warp_excl_scan((unsigned)((my_kend - my_kb + 31) >> 5), steps);
+    if (lane == 0) {
+      if (steps > 0) {
+        const unsigned long long s0 = atomicAdd(mc.head, (unsigned long long)steps);
+        slot = (long long)(s0 + steps) <= mc.cap ? (long long)s0 : -1;
       }
-      const unsigned b64 = __ballot_sync(0xffffffffu, hi), b32 = __ballot_sync(0xffffffffu, lo);
+      mc.slot[task] = slot;
+    }
+    slot = __shfl_sync(0xffffffffu, slot, 0);
+  } else {
+    slot = mc.slot[task];
+  }
+  long long step = 0;
+  for (int bk = 0; bk < CQG_NBUCKET; ++bk) {
+    const int kb = __shfl_sync(0xffffffffu, my_kb, bk), kend = __shfl_sync(0xffffffffu, my_kend, bk);
+    for (int k0 = kb; k0 < kend; k0 += 32, ++step) {
+      const int ket = k0 + lane;
+      unsigned b64, b32;
+      if (FILL && slot >= 0) {   // survivors from the count pass
+        const uint2 m = mc.masks[slot + step];
+        b64 = m.x;
+        b32 = m.y;
+      } else {
+        bool hi = false, lo = false;
+        if (ket < kend) {
+          const double bnd = quartet_bound(col1, col2, m12, Mpair[ket], shoff, P.sh[ket], qb, P.Q[ket]);
+          const bool pass = bnd >= thresh;
+          lo = pass && bnd < cut32;
+          hi = pass && !lo;
+        }
+        b64 = __ballot_sync(0xffffffffu, hi);
+        b32 = __ballot_sync(0xffffffffu, lo);
+        if (!FILL && slot >= 0 && lane == 0) mc.masks[slot + step] = make_uint2(b64, b32);
+      }
+      const bool hi = (b64 >> lane) & 1u, lo = (b32 >> lane) & 1u;
       if (FILL) {
         if (hi && dop[0]) {
           const long long pos = base[0] + cpart[0] + __popc(b64 & below);
@@ -561,7 +618,7 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
                                                   const long long *__restrict__ off, uint2 *__restrict__ qlist,
                                                   unsigned short *__restrict__ qmask,
                                                   unsigned long long *__restrict__ blkacc, long long vt0,
-                                                  long long vt1, long long obase, long long cap) {
+                                                  long long vt1, long long obase, long long cap, MaskCache mc) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= ntask) return;
@@ -589,8 +646,8 @@ __global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pair
     screen_group_task<FILL>(bt, blk, t, P, MT, Mpair, mols, shmol, mm, thresh, cut32, dop, base, cpart, qlist,
                             qmask, cap, ty);
   else
-    screen_pair_task<FILL>(bt, blk, t, P, M, MT, Mpair, mols, shmol, mm, thresh, cut32, dop, base, cpart, qlist,
-                           cap, ty);
+    screen_pair_task<FILL>(bt, blk, t, warp, P, M, MT, Mpair, mols, shmol, mm, thresh, cut32, dop, base, cpart,
+                           qlist, cap, mc, ty);
   if (!FILL) {
     for (int o = 16; o > 0; o >>= 1) {
       ty.km64 += __shfl_xor_sync(0xffffffffu, ty.km64, o);
@@ -1598,6 +1655,11 @@ struct cqg_ctx {
   DevBuf<double> d_pair_Qc, d_gQ, d_gw;
   DevBuf<PrimPair> d_gprim;
   DevBuf<unsigned short> d_qmask;     // member masks, parallel to d_qlist
+  // survivor-mask cache of the screening passes (MaskCache): steps, head, per-task slots
+  DevBuf<uint2> d_masks;
+  DevBuf<unsigned long long> d_mhead;
+  DevBuf<long long> d_mslot;
+  long long mask_steps_used = 0;      // steps the last count pass asked for
   cudaEvent_t ev[4 + 2 * CQG_NQC + 2];
   bool events = false;
   cqg_stats stats;
@@ -1666,6 +1728,15 @@ static cudaError_t launch_schwarz(cqg_ctx *ctx, Pairs P, Shells S, int beg, int 
     k_schwarz<LA, LB><<<(n + 127) / 128, 128>>>(P, S, ctx->d_boys.p, beg, end, Q);
     return cudaGetLastError();
   }
+}
+
+static inline MaskCache make_mask_cache(cqg_ctx *ctx) {
+  MaskCache mc;
+  mc.masks = ctx->d_masks.p;
+  mc.head = ctx->d_mhead.p;
+  mc.slot = ctx->d_mslot.p;
+  mc.cap = (long long)ctx->d_masks.n;
+  return mc;
 }
 
 static inline Pairs make_pairs(cqg_ctx *ctx) {
