@@ -185,7 +185,7 @@ def _aname(members, mb, mk, i):
     return "acc%d_%d_%d" % (mb, mk, i) if members else "acc%d" % i
 
 
-def _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members=None, nkt=1):
+def _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members=None, nkt=1, prefetch=True):
     """One pass over `nbt` bra primitive pairs starting at bra[ib]: their E coefficients,
     the ket loop (each ket primitive pair loaded and its E coefficients built once for
     all nbt bra primitives; with nkt > 1, nkt ket primitive pairs per iteration, whose
@@ -323,13 +323,18 @@ def _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members=No
         g.w("PrimPair pk_next;")
         g.w("if (ik < nket) pk_next = ket[ik];")
         g.w("for (; ik < nket; ++ik) {")
-    else:
+    elif prefetch:
         g.w("PrimPair pk_next;")
         g.w("if (nket > 0) pk_next = ket[0];")
         g.w("for (int ik = 0; ik < nket; ++ik) {")
+    else:
+        g.w("for (int ik = 0; ik < nket; ++ik) {")
     g.ind += 1
-    g.w("const PrimPair pk = pk_next;")
-    g.w("if (ik + 1 < nket) pk_next = ket[ik + 1];")
+    if prefetch or nkt > 1:
+        g.w("const PrimPair pk = pk_next;")
+        g.w("if (ik + 1 < nket) pk_next = ket[ik + 1];")
+    else:
+        g.w("const PrimPair pk = ket[ik];")
     kterms = ket_quantities("k", "q", "kc_")
     for j in range(nbt):
         chain(j, "k", "q", kterms, "r%d_" % j)
@@ -362,10 +367,10 @@ def _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members=No
                 ai += 1
 
 
-def gen_class(la, lb, lc, ld, pa, pb, pc, pd, nbt=1, members=None, nkt=1):
+def gen_class(la, lb, lc, ld, pa, pb, pc, pd, nbt=1, members=None, nkt=1, prefetch=True):
     """Device function of one class; nbt > 1 walks the bra primitive pairs nbt at a time
     (each ket primitive pair is then read once per nbt bra primitives), with a one-at-a-time
-    loop for the remainder.
+    loop for the remainder.  prefetch loads the next ket primitive pair one step ahead.
 
     members = (mb, mk) emits eri_gc_<class>_<mb>x<mk> instead: mb bra and mk ket sibling
     pairs (same centres, angular momenta and exponents, different contraction coefficients)
@@ -399,12 +404,12 @@ def gen_class(la, lb, lc, ld, pa, pb, pc, pd, nbt=1, members=None, nkt=1):
     if nbt > 1:
         g.w("for (; ib + %d < nbra; ib += %d) {" % (nbt - 1, nbt))
         g.ind += 1
-        _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members, nkt)
+        _emit_tile(g, nbt, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members, nkt, prefetch)
         g.ind -= 1
         g.w("}")
     g.w("for (; ib < nbra; ++ib) {")
     g.ind += 1
-    _emit_tile(g, 1, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members, nkt)
+    _emit_tile(g, 1, la, lb, lc, ld, ca, cb, cc, cd, hp, hidx, ncd, members, nkt, prefetch)
     g.ind -= 1
     g.w("}")
     # spherical transform, axis by axis: cart arrays named by index tuples
@@ -489,6 +494,13 @@ BRA_TILE = {(0, 0, 0, 0): 4}
 # 18 % slower; so no class uses it.
 KET_TILE = {}
 
+# classes whose ket loop loads each primitive pair where it is used instead of one step
+# ahead.  Measured on (H2O)_32 cc-pVDZ with every per-thread class both ways: the prefetch
+# is worth 0.2-0.45 ms per class on the s and p classes ((ps|ss) 13.04 against 13.48 ms even
+# though the variant without it fits five CTAs per SM instead of four), and costs 0.03-0.13
+# ms on these, the spilling classes among them.
+NO_KET_PREFETCH = {(1, 1, 1, 1), (2, 0, 0, 0), (2, 0, 1, 1), (2, 0, 2, 0), (2, 1, 2, 0), (2, 2, 1, 0)}
+
 
 # Sibling-group classes of the engine (la, lb, lc, ld, mb, mk): their lists hold entries of
 # one bra and one ket group of sibling pairs (same centres, angular momenta and exponents),
@@ -539,7 +551,8 @@ def main(path, maxl=2):
         if (la, lb, lc, ld) in WARP_CLASSES:
             continue
         _, code = gen_class(la, lb, lc, ld, la > 1, lb > 1, lc > 1, ld > 1,
-                            nbt=BRA_TILE.get((la, lb, lc, ld), 1), nkt=KET_TILE.get((la, lb, lc, ld), 1))
+                            nbt=BRA_TILE.get((la, lb, lc, ld), 1), nkt=KET_TILE.get((la, lb, lc, ld), 1),
+                            prefetch=(la, lb, lc, ld) not in NO_KET_PREFETCH)
         parts.append(code)
         parts.append("template <> struct EriClass<%d, %d, %d, %d> {" % (la, lb, lc, ld))
         parts.append("  template <typename T> static __device__ __forceinline__ void run(const PrimPair* bra, int nbra,"
