@@ -19,7 +19,7 @@ struct __align__(16) PrimPair {
 //                 (grid step 0.1, F_{n}'(T) = -F_{n+1}(T)), then downward recursion
 //                 F_m = (2T F_{m+1} + e^-T) / (2m+1).
 //  T >= BOYS_TMAX: F_0 = sqrt(pi/T)/2 (erf(sqrt T) = 1 to 2e-17 there), then upward
-//                 recursion F_{m+1} = ((2m+1) F_m - e^-T) / (2T).
+//                 recursion F_{m+1} = ((2m+1) F_m - e^-T) / (2T); T^(-1/2) from rsqrt.
 // Table layout: tab[i * BOYS_NORD + n] = F_n(0.1 i), i = 0..BOYS_NT-1, followed by
 // tab[BOYS_NT * BOYS_NORD + i] = exp(-0.1 i).
 #define BOYS_TMAX 36.0
@@ -59,10 +59,12 @@ __device__ __forceinline__ void boys_eval(double T, const double* __restrict__ t
       for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * (1.0 / (2 * m + 1));
     }
   } else {
-    F[0] = 0.5 * sqrt(3.141592653589793 / T);
+    // F_0 = (sqrt(pi) / 2) T^(-1/2) and 1 / (2T) from one reciprocal square root
+    const double r = rsqrt(T);
+    F[0] = 0.88622692545275801 * r;
     if (L > 0) {
       const double e = exp(-T);
-      const double i2t = 0.5 / T;
+      const double i2t = 0.5 * r * r;
 #pragma unroll
       for (int m = 0; m < L; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) * i2t;
     }
@@ -117,10 +119,12 @@ __device__ __forceinline__ void boys_eval_sm(double T, const double *s, double *
       for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * (1.0 / (2 * m + 1));
     }
   } else {
-    F[0] = 0.5 * sqrt(3.141592653589793 / T);
+    // F_0 = (sqrt(pi) / 2) T^(-1/2) and 1 / (2T) from one reciprocal square root
+    const double r = rsqrt(T);
+    F[0] = 0.88622692545275801 * r;
     if (L > 0) {
       const double e = exp(-T);
-      const double i2t = 0.5 / T;
+      const double i2t = 0.5 * r * r;
 #pragma unroll
       for (int m = 0; m < L; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) * i2t;
     }
