@@ -123,7 +123,9 @@ __device__ __forceinline__ void boys_eval_sm(double T, const double *s, double *
     const double r = rsqrt(T);
     F[0] = 0.88622692545275801 * r;
     if (L > 0) {
-      const double e = exp(-T);
+      // F_1 = (F_0 - e^-T) / (2T): for T >= 36, e^-T / F_0 < 1.6e-15, within the Taylor
+      // branch's accuracy, so L = 1 drops it; higher orders need it
+      const double e = L == 1 ? 0.0 : exp(-T);
       const double i2t = 0.5 * r * r;
 #pragma unroll
       for (int m = 0; m < L; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) * i2t;
