@@ -483,9 +483,13 @@ WARP_CLASSES = {q for q in quartet_classes(3)
 
 # classes whose bra primitive pairs are walked several at a time, so that each ket
 # primitive pair read serves several primitive quartets.  Measured on (H2O)_32 cc-pVDZ:
-# (ss|ss) 12.3 -> 8.1 ms with 4 at a time; (ps|ss), (ps|ps), (pp|ss), (ds|ss) get 4-15 %
-# slower with 2 (register pressure), so they keep one.
-BRA_TILE = {(0, 0, 0, 0): 4}
+# (ss|ss) 12.3 -> 8.1 ms with 4 at a time (8: 12 % slower); (ps|ss) 12.85 -> 10.05 ms with 3
+# (156 registers, three CTAs per SM; 2: 10.58, 4: 11.42 ms).  (ps|ps), (pp|ss), (ds|ss),
+# (dp|ss) get 6-29 % slower with 2 (register pressure), so they keep one.
+BRA_TILE = {(0, 0, 0, 0): 4, (1, 0, 0, 0): 3}
+# the same for the sibling forms (members_header), whose member accumulators leave less room:
+# (ps|ss) 2 x 4 with three bra primitives at a time reaches 255 registers and spills
+GC_BRA_TILE = {(0, 0, 0, 0): 4}
 
 # classes whose ket primitive pairs are walked several at a time within each bra primitive
 # (independent chains of Boys values and R recursion per iteration).  Measured on (H2O)_32
@@ -523,7 +527,7 @@ def members_header(specs):
              ""]
     for (la, lb, lc, ld, mb, mk) in specs:
         name, code = gen_class(la, lb, lc, ld, la > 1, lb > 1, lc > 1, ld > 1,
-                               nbt=BRA_TILE.get((la, lb, lc, ld), 1), members=(mb, mk))
+                               nbt=GC_BRA_TILE.get((la, lb, lc, ld), 1), members=(mb, mk))
         parts.append(code)
         parts.append("template <> struct EriClassGC<%d, %d, %d, %d, %d, %d> {" % (la, lb, lc, ld, mb, mk))
         parts.append("  template <typename T> static __device__ __forceinline__ void run(const PrimPair* bra,"
