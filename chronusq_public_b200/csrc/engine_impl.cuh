@@ -609,8 +609,10 @@ __device__ __forceinline__ void screen_group_task(const BlockTable &bt, int blk,
   }
 }
 
+// Four CTAs of 256 threads per SM (64 registers; a few bytes of spills): the latency-bound
+// screening runs 3.54 -> 3.02 ms per (H2O)_32 build against three CTAs at 80 registers.
 template <bool FILL>
-__global__ void __launch_bounds__(256) k_quartets(BlockTable bt, int ntask, Pairs P, const double *__restrict__ M,
+__global__ void __launch_bounds__(256, 4) k_quartets(BlockTable bt, int ntask, Pairs P, const double *__restrict__ M,
                                                   const double *__restrict__ MT, const double *__restrict__ Mpair,
                                                   Mols mols, const int *__restrict__ shmol,
                                                   const double *__restrict__ Mmax, double thresh,
