@@ -1,4 +1,4 @@
-"""The C++ change that a ChronusQ maintainer adds (the cpp block of INTEGRATION.md) is
+"""The C++ change that a ChronusQ maintainer adds (the cpp block of the integration guide) is
 compiled against stand-ins with the reference's names and signatures, linked to
 libcqgpu.so, and run.  Without a GPU the call reaches cqg_create and reports its failure
 through CErr; with one it completes and gives J of a one-function basis."""
